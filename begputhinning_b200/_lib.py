@@ -1,0 +1,122 @@
+"""Loader for the native library ``libbgt.so`` (ctypes over the C ABI in
+``include/bgt_capi.h``).  There is no fallback: if the library cannot be
+loaded, every entry point raises."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libbgt.so")
+SYNTH_PATH = os.path.join(PKG, "libbgt_synth.so")
+
+# names declared in include/bgt_capi.h (kept in sync by tests/test_capi_symbols.py)
+EXPORTS = [
+    "bgt_ctx_create", "bgt_ctx_destroy", "bgt_ctx_set_stream", "bgt_last_error", "bgt_version",
+    "bgt_thin2d", "bgt_thin3d", "bgt_thin2d_device", "bgt_thin3d_device",
+    "bgt_centerline2d", "bgt_centerline3d", "bgt_free",
+    "bgt_segments2d_device", "bgt_segments3d_device",
+    "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
+    "bgt_batch_set_io", "bgt_batch_run", "bgt_batch_instance_stats", "bgt_batch_device_bytes",
+    "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe",
+]
+
+
+class BGTError(RuntimeError):
+    """A C-ABI call returned a nonzero bgt_status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"bgt error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+_synth = None
+
+P = C.c_void_p
+I = C.c_int
+PP = C.POINTER(C.c_void_p)
+
+
+def _declare(L):
+    vp, ip, up = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint)
+    fpp = C.POINTER(C.POINTER(C.c_float))
+    upp = C.POINTER(C.POINTER(C.c_uint))
+    sig = {
+        "bgt_ctx_create": [I, C.POINTER(vp)],
+        "bgt_ctx_destroy": [vp],
+        "bgt_ctx_set_stream": [vp, vp],
+        "bgt_version": [],
+        "bgt_thin2d": [vp, I, vp, I, I, vp],
+        "bgt_thin3d": [vp, I, vp, I, I, I, vp],
+        "bgt_thin2d_device": [vp, I, vp, I, I, vp],
+        "bgt_thin3d_device": [vp, I, vp, I, I, I, vp],
+        "bgt_centerline2d": [vp, I, vp, I, I, I, I, fpp, fpp, upp, up],
+        "bgt_centerline3d": [vp, I, vp, I, I, I, I, I, fpp, fpp, fpp, upp, up],
+        "bgt_segments2d_device": [vp, I, vp, I, I, C.POINTER(C.POINTER(C.c_int32)),
+                                  C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.POINTER(C.c_int16)),
+                                  C.POINTER(C.POINTER(C.c_int16)), ip, ip],
+        "bgt_segments3d_device": [vp, I, vp, I, I, I, C.POINTER(C.POINTER(C.c_int32)),
+                                  C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(C.POINTER(C.c_int16)),
+                                  C.POINTER(C.POINTER(C.c_int16)), C.POINTER(C.POINTER(C.c_int16)), ip, ip],
+        "bgt_batch_create": [vp, C.POINTER(vp)],
+        "bgt_batch_destroy": [vp],
+        "bgt_batch_add2d": [vp, I, I, I, ip],
+        "bgt_batch_add3d": [vp, I, I, I, I, ip],
+        "bgt_batch_finalize": [vp],
+        "bgt_batch_set_io": [vp, I, I, vp, vp],
+        "bgt_batch_run": [vp, I, I],
+        "bgt_batch_instance_stats": [vp, I, ip, ip, ip],
+        "bgt_batch_device_bytes": [vp, C.POINTER(C.c_size_t)],
+        "bgt_tune_class": [I, I, I, I],
+        "bgt_tune_set": [I, I, I],
+        "bgt_tune_get": [I, I, ip],
+        "bgt_cfg_list": [I, ip, I, ip],
+        "bgt_cfg_describe": [I, ip, ip, ip, ip, ip, ip],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.bgt_last_error.argtypes = []
+    L.bgt_last_error.restype = C.c_char_p
+    L.bgt_free.argtypes = [vp]
+    L.bgt_free.restype = None
+
+
+def lib():
+    """The loaded libbgt.so (raises if it is missing: there is no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"native library {LIB_PATH} not built; run python -m begputhinning_b200.build")
+        L = C.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise BGTError(rc, lib().bgt_last_error().decode(errors="replace"))
+
+
+def synth():
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_PATH):
+            raise ImportError(f"{SYNTH_PATH} not built; run python -m begputhinning_b200.build")
+        L = C.CDLL(SYNTH_PATH)
+        u8p = C.POINTER(C.c_uint8)
+        dp = C.POINTER(C.c_double)
+        d = C.c_double
+        L.bgt_synth_uniform.argtypes = [C.c_uint64, C.c_int64, dp]
+        L.bgt_synth_render_strokes2d.argtypes = [I, I, I, dp, dp, u8p]
+        L.bgt_synth_strokes2d.argtypes = [C.c_uint64, I, I, I, d, d, u8p]
+        L.bgt_synth_vessels2d.argtypes = [C.c_uint64, I, I, I, I, d, d, d, d, d, d, d, I, d, d, u8p]
+        L.bgt_synth_trees3d.argtypes = [C.c_uint64, I, I, I, I, I, d, d, d, d, d, d, I, d, d, u8p]
+        for n in ["bgt_synth_uniform", "bgt_synth_render_strokes2d", "bgt_synth_strokes2d",
+                  "bgt_synth_vessels2d", "bgt_synth_trees3d"]:
+            getattr(L, n).restype = None
+        _synth = L
+    return _synth

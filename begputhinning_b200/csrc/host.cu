@@ -1,0 +1,643 @@
+// host.cu -- host side of the C ABI: contexts, batches (device pool layout,
+// TMA tensor maps, the persistent engine and the plain per-pass path, CUDA
+// graph replay) and the drop-in thinning entry points.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include <cudaTypedefs.h>
+
+#include "host.h"
+#include "kernels.cuh"
+
+using namespace bgt;
+
+// ------------------------------------------------------------ errors -------
+static thread_local std::string g_err;
+
+int bgt::fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int bgt::cuda_fail(cudaError_t e, const char *what)
+{
+    return fail(e == cudaErrorMemoryAllocation ? BGT_ERR_NOMEM : BGT_ERR_CUDA, "%s: %s (%d)", what,
+                cudaGetErrorString(e), (int)e);
+}
+
+extern "C" const char *bgt_last_error(void) { return g_err.c_str(); }
+extern "C" int bgt_version(void) { return 100; }
+
+size_t bgt::dtype_size(int dtype)
+{
+    switch (dtype) {
+    case BGT_U8: case BGT_I8: case BGT_CHAR: case BGT_BOOL: return 1;
+    case BGT_U16: case BGT_I16: return 2;
+    case BGT_U32: case BGT_I32: case BGT_F32: return 4;
+    case BGT_F64: return 8;
+    default: return 0;
+    }
+}
+
+// ------------------------------------------------------------ context ------
+extern "C" int bgt_ctx_create(int device, bgt_ctx **out)
+{
+    if (!out) return fail(BGT_ERR_ARG, "bgt_ctx_create: out is null");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    bgt_ctx *c = new bgt_ctx();
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "cudaStreamCreate");
+    }
+    c->stream = c->own;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    *out = c;
+    return BGT_OK;
+}
+
+extern "C" int bgt_ctx_destroy(bgt_ctx *c)
+{
+    if (!c) return BGT_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto &kv : c->cache) bgt_batch_destroy(kv.second);
+    c->cache.clear();
+    for (auto &p : c->scratch) cudaFree(p.ptr);
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+    return BGT_OK;
+}
+
+extern "C" int bgt_ctx_set_stream(bgt_ctx *c, void *stream)
+{
+    if (!c) return fail(BGT_ERR_ARG, "null context");
+    c->stream = stream ? (cudaStream_t)stream : c->own;
+    for (auto &kv : c->cache) kv.second->graph_valid = false;
+    return BGT_OK;
+}
+
+// Named resident scratch buffer of at least `bytes` (grown, never shrunk).
+int bgt::ctx_scratch(bgt_ctx *c, int slot, size_t bytes, void **out)
+{
+    if ((int)c->scratch.size() <= slot) c->scratch.resize(slot + 1);
+    Scratch &s = c->scratch[slot];
+    if (s.bytes < bytes) {
+        if (s.ptr) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(s.ptr);
+            s.ptr = nullptr;
+            s.bytes = 0;
+        }
+        size_t nb = std::max(bytes, (size_t)4096);
+        cudaError_t e = cudaMalloc(&s.ptr, nb);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(scratch)");
+        s.bytes = nb;
+    }
+    *out = s.ptr;
+    return BGT_OK;
+}
+
+// ------------------------------------------------------------ tensor maps --
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+static int encode_map(CUtensorMap *m, const Inst &in, const CfgInfo &c, uint32_t *base)
+{
+    auto enc = get_encode();
+    if (!enc) return fail(BGT_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[3] = {(cuuint64_t)in.P, (cuuint64_t)in.H, (cuuint64_t)in.D};
+    cuuint64_t strides[2] = {(cuuint64_t)in.P * 4, (cuuint64_t)in.P * in.H * 4};
+    cuuint32_t box[3] = {(cuuint32_t)c.box[0], (cuuint32_t)c.box[1], (cuuint32_t)c.box[2]};
+    cuuint32_t estr[3] = {1, 1, 1};
+    const cuuint32_t rank = in.dims == 2 ? 2 : 3;
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, rank, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(BGT_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) P=%d H=%d D=%d box=%u,%u,%u", (int)r, in.P,
+                    in.H, in.D, box[0], box[1], box[2]);
+    return BGT_OK;
+}
+
+// ------------------------------------------------------------ autotune ----
+// Default tile configuration by shape; the autotuner (tune.cpp) may override
+// through bgt::tuned_cfg.
+int bgt::default_cfg(int dims, int W, int H, int D)
+{
+    (void)H;
+    (void)D;
+    if (dims == 3) return 17;
+    return W > 768 ? 6 : 2;
+}
+
+// ------------------------------------------------------------ batch -------
+extern "C" int bgt_batch_create(bgt_ctx *ctx, bgt_batch **out)
+{
+    if (!ctx || !out) return fail(BGT_ERR_ARG, "bgt_batch_create: null argument");
+    bgt_batch *b = new bgt_batch();
+    b->ctx = ctx;
+    *out = b;
+    return BGT_OK;
+}
+
+static void batch_free_device(bgt_batch *b)
+{
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+    b->graph_valid = false;
+    if (b->pool) cudaFree(b->pool);
+    b->pool = nullptr;
+}
+
+extern "C" int bgt_batch_destroy(bgt_batch *b)
+{
+    if (!b) return BGT_OK;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    batch_free_device(b);
+    delete b;
+    return BGT_OK;
+}
+
+static int batch_add(bgt_batch *b, int dims, int W, int H, int D, int cfg, int *id)
+{
+    if (!b) return fail(BGT_ERR_ARG, "null batch");
+    if (b->finalized) return fail(BGT_ERR_STATE, "batch already finalized");
+    if (W < 1 || H < 1 || D < 1 || W > 32767 || H > 32767 || D > 32767)
+        return fail(BGT_ERR_ARG, "size %dx%dx%d out of range (1..32767 per axis)", W, H, D);
+    if (cfg >= 0) {
+        const CfgInfo *c = cfg_info(cfg);
+        if (!c || c->dims != dims) return fail(BGT_ERR_ARG, "configuration %d is not a %dD configuration", cfg, dims);
+    }
+    BatchItem it;
+    it.dims = dims;
+    it.W = W;
+    it.H = H;
+    it.D = D;
+    it.cfg = cfg;
+    b->items.push_back(it);
+    if (id) *id = (int)b->items.size() - 1;
+    return BGT_OK;
+}
+
+extern "C" int bgt_batch_add2d(bgt_batch *b, int w, int h, int cfg, int *id) { return batch_add(b, 2, w, h, 1, cfg, id); }
+extern "C" int bgt_batch_add3d(bgt_batch *b, int w, int h, int d, int cfg, int *id)
+{
+    return batch_add(b, 3, w, h, d, cfg, id);
+}
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+extern "C" int bgt_batch_finalize(bgt_batch *b)
+{
+    if (!b) return fail(BGT_ERR_ARG, "null batch");
+    if (b->finalized) return BGT_OK;
+    if (b->items.empty()) return fail(BGT_ERR_STATE, "empty batch");
+    cudaSetDevice(b->ctx->device);
+    const int N = (int)b->items.size();
+    b->h.assign(N, Inst());
+    size_t off = 0;
+    size_t total_tiles = 0;
+    int max_smem = 0;
+    struct Offs { size_t b0, b1, uni, lc, act, list; };
+    std::vector<Offs> offs(N);
+    for (int i = 0; i < N; i++) {
+        BatchItem &it = b->items[i];
+        if (it.cfg < 0) it.cfg = tuned_cfg(it.dims, it.W, it.H, it.D);
+        const CfgInfo &c = *cfg_info(it.cfg);
+        Inst &in = b->h[i];
+        memset(&in, 0, sizeof(in));
+        in.dims = it.dims;
+        in.W = it.W;
+        in.H = it.H;
+        in.D = it.D;
+        in.P = (int)align_up((size_t)(it.W + 31) / 32, 4);
+        in.cfg = it.cfg;
+        in.TW = c.TW;
+        in.TH = c.TH;
+        in.TZ = c.TZc;
+        in.k = c.k;
+        in.window = std::max(1, (4 + c.k - 1) / c.k);
+        const int wwords = (it.W + 31) / 32;
+        in.tiles_x = (wwords + c.TW - 1) / c.TW;
+        in.tiles_y = (it.H + c.TH - 1) / c.TH;
+        in.tiles_z = (it.D + c.TZc - 1) / c.TZc;
+        in.ntiles = in.tiles_x * in.tiles_y * in.tiles_z;
+        const int maxdim = std::max(it.W, std::max(it.H, it.D));
+        const int passes_per_iter = it.dims == 3 ? 6 : std::max(1, 4 / c.k);
+        in.pass_cap = (maxdim + 16) * passes_per_iter + 64;
+        const size_t words = (size_t)in.P * it.H * it.D;
+        Offs &o = offs[i];
+        o.b0 = off; off = align_up(off + words * 4, 256);
+        o.b1 = off; off = align_up(off + words * 4, 256);
+        if (it.dims == 3) { o.uni = off; off = align_up(off + words * 4, 256); }
+        o.lc = off; off = align_up(off + (size_t)in.ntiles * 4, 256);
+        o.act = off; off = align_up(off + (size_t)in.ntiles, 256);
+        o.list = off; off = align_up(off + (size_t)in.ntiles * 4, 256);
+        total_tiles += in.ntiles;
+        max_smem = std::max(max_smem, c.smem);
+    }
+    // scheduler + ring + instance table + tensor maps + flags
+    const unsigned cap = (unsigned)(total_tiles + 1024);
+    const size_t off_sched = off; off = align_up(off + sizeof(Sched), 256);
+    const size_t off_seq = off; off = align_up(off + (size_t)cap * 4, 256);
+    const size_t off_item = off; off = align_up(off + (size_t)cap * sizeof(int4), 256);
+    const size_t off_inst = off; off = align_up(off + (size_t)N * sizeof(Inst), 256);
+    const size_t off_tmap = off; off = align_up(off + (size_t)N * 2 * sizeof(CUtensorMap), 256);
+    const size_t off_flag = off; off = align_up(off + 64, 256);
+    cudaError_t e = cudaMalloc(&b->pool, off);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch pool)");
+    b->pool_bytes = off;
+    char *P = (char *)b->pool;
+    b->d_sched = (Sched *)(P + off_sched);
+    b->d_seq = (unsigned *)(P + off_seq);
+    b->d_item = (int4 *)(P + off_item);
+    b->d_insts = (Inst *)(P + off_inst);
+    b->d_tmaps = (CUtensorMap *)(P + off_tmap);
+    b->d_flag = (int *)(P + off_flag);
+    b->cap = cap;
+    std::vector<CUtensorMap> maps((size_t)N * 2);
+    for (int i = 0; i < N; i++) {
+        Inst &in = b->h[i];
+        const Offs &o = offs[i];
+        in.buf[0] = (uint32_t *)(P + o.b0);
+        in.buf[1] = (uint32_t *)(P + o.b1);
+        in.uni = in.dims == 3 ? (uint32_t *)(P + o.uni) : nullptr;
+        in.lc = (int *)(P + o.lc);
+        in.act = (uint8_t *)(P + o.act);
+        in.list = (int *)(P + o.list);
+        in.tmap = b->d_tmaps + 2 * i;
+        const CfgInfo &c = *cfg_info(in.cfg);
+        int rc = encode_map(&maps[2 * i], in, c, in.buf[0]);
+        if (rc == BGT_OK) rc = encode_map(&maps[2 * i + 1], in, c, in.buf[1]);
+        if (rc != BGT_OK) {
+            batch_free_device(b);
+            return rc;
+        }
+    }
+    e = cudaMemcpy(b->d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_insts, b->h.data(), (size_t)N * sizeof(Inst), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        batch_free_device(b);
+        return cuda_fail(e, "cudaMemcpy(batch tables)");
+    }
+    b->smem = max_smem;
+    e = engine_set_smem(std::max(max_smem, 48 * 1024));
+    if (e != cudaSuccess) {
+        batch_free_device(b);
+        return cuda_fail(e, "cudaFuncSetAttribute");
+    }
+    const int per_sm = std::max(1, engine_max_blocks_per_sm(max_smem));
+    b->grid = b->ctx->sms * per_sm;
+    b->io.assign(N, IO());
+    b->stats.assign(N, Stat());
+    b->finalized = true;
+    return BGT_OK;
+}
+
+extern "C" int bgt_batch_set_io(bgt_batch *b, int id, int dtype, const void *d_in, void *d_out)
+{
+    if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    if (id < 0 || id >= (int)b->items.size()) return fail(BGT_ERR_ARG, "bad instance id %d", id);
+    if (dtype_size(dtype) == 0) return fail(BGT_ERR_ARG, "bad dtype %d", dtype);
+    IO &io = b->io[id];
+    if (io.in != d_in || io.out != d_out || io.dtype != dtype) b->graph_valid = false;
+    io.dtype = dtype;
+    io.in = d_in;
+    io.out = d_out;
+    return BGT_OK;
+}
+
+int bgt::batch_set_input_extent(bgt_batch *b, int id, int inW, int inH, int inD)
+{
+    if (!b || !b->finalized || id < 0 || id >= (int)b->items.size()) return fail(BGT_ERR_ARG, "bad batch/id");
+    const Inst &in = b->h[id];
+    if (inW > in.W || inH > in.H || inD > in.D) return fail(BGT_ERR_ARG, "input extent larger than the instance");
+    IO &io = b->io[id];
+    if (io.inW != inW || io.inH != inH || io.inD != inD) b->graph_valid = false;
+    io.inW = inW;
+    io.inH = inH;
+    io.inD = inD;
+    return BGT_OK;
+}
+
+__global__ void sched_reset_kernel(Sched *S, unsigned *seq, int4 *item, unsigned cap, long long timeout_ns)
+{
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        S->head = 0;
+        S->tail = 0;
+        S->live = 0;
+        S->status = 0;
+        S->cap = cap;
+        S->seq = seq;
+        S->item = item;
+        S->timeout_ns = timeout_ns;
+    }
+    for (unsigned s = i; s < cap; s += gridDim.x * blockDim.x) seq[s] = s;
+}
+
+// Stream-ordered sequence of the engine run (capturable).
+static int enqueue_engine(bgt_batch *b, cudaStream_t st)
+{
+    const int N = (int)b->items.size();
+    cudaError_t e;
+    for (int i = 0; i < N; i++) {
+        const Inst &in = b->h[i];
+        const IO &io = b->io[i];
+        if (!io.in) return fail(BGT_ERR_STATE, "instance %d has no input", i);
+        e = launch_pack(io.dtype, in.dims == 2 ? 0 : 1, io.in, io.inW ? io.inW : in.W, io.inH ? io.inH : in.H,
+                        io.inD ? io.inD : in.D, in.W, in.H, in.D, in.P, in.buf[0], in.buf[1], st);
+        if (e != cudaSuccess) return cuda_fail(e, "pack");
+        e = launch_tile_init(b->d_insts + i, in, nullptr, st);
+        if (e != cudaSuccess) return cuda_fail(e, "tile init");
+    }
+    sched_reset_kernel<<<std::min<unsigned>(1024, (b->cap + 255) / 256), 256, 0, st>>>(
+        b->d_sched, b->d_seq, b->d_item, b->cap, 20000000000LL);
+    e = launch_engine(b->grid, b->smem, b->d_insts, N, b->d_sched, st);
+    if (e != cudaSuccess) return cuda_fail(e, "engine launch");
+    for (int i = 0; i < N; i++) {
+        const Inst &in = b->h[i];
+        const IO &io = b->io[i];
+        if (!io.out) continue;
+        e = launch_unpack(io.dtype, in.buf[0], in.W, in.H, in.D, in.P, io.out, st);
+        if (e != cudaSuccess) return cuda_fail(e, "unpack");
+    }
+    return BGT_OK;
+}
+
+static int run_engine(bgt_batch *b, int use_graph)
+{
+    cudaStream_t st = b->ctx->stream;
+    int rc;
+    if (use_graph) {
+        if (!b->graph_valid) {
+            if (b->gexec) cudaGraphExecDestroy(b->gexec);
+            b->gexec = nullptr;
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+            rc = enqueue_engine(b, st);
+            e = cudaStreamEndCapture(st, &g);
+            if (rc != BGT_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&b->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+            b->graph_valid = true;
+        }
+        cudaError_t e = cudaGraphLaunch(b->gexec, st);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+    } else {
+        rc = enqueue_engine(b, st);
+        if (rc != BGT_OK) return rc;
+    }
+    b->stats_valid = false;
+    b->last_mode = 0;
+    return BGT_OK;
+}
+
+static int run_plain(bgt_batch *b)
+{
+    cudaStream_t st = b->ctx->stream;
+    const int N = (int)b->items.size();
+    cudaError_t e;
+    int *h_flag = nullptr;
+    e = cudaMallocHost(&h_flag, 64);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+    int rc = BGT_OK;
+    // per-launch status word lives in the scheduler block
+    int *d_err = &b->d_sched->status;
+    cudaMemsetAsync(d_err, 0, sizeof(int), st);
+    for (int i = 0; i < N && rc == BGT_OK; i++) {
+        const Inst &in = b->h[i];
+        const IO &io = b->io[i];
+        if (!io.in) { rc = fail(BGT_ERR_STATE, "instance %d has no input", i); break; }
+        e = launch_pack(io.dtype, in.dims == 2 ? 0 : 1, io.in, io.inW ? io.inW : in.W, io.inH ? io.inH : in.H,
+                        io.inD ? io.inD : in.D, in.W, in.H, in.D, in.P, in.buf[0], in.buf[1], st);
+        if (e == cudaSuccess) e = launch_tile_init(b->d_insts + i, in, nullptr, st);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "pack"); break; }
+        int last_change = -1;  // tiles start "changed just before pass 0"
+        int q = 0;
+        int converged = 0;
+        for (; q < in.pass_cap; q++) {
+            cudaMemsetAsync(b->d_flag, 0, sizeof(int), st);
+            e = launch_plain_pass(in.cfg, b->d_insts + i, in.ntiles, q, b->d_flag, d_err, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h_flag, b->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) { rc = cuda_fail(e, "plain pass"); break; }
+            if (h_flag[0]) last_change = q;
+            if (in.dims == 2) {
+                if (q - last_change >= in.window) { converged = 1; q++; break; }
+            } else if (q % 6 == 5 && last_change < q - 5) {
+                converged = 1;
+                q++;
+                break;
+            }
+        }
+        b->stats[i].passes = q;
+        b->stats[i].converged = converged ? 1 : -1;
+        if (rc == BGT_OK && !converged) rc = fail(BGT_ERR_LIMIT, "instance %d hit the pass cap", i);
+        if (rc == BGT_OK && io.out) {
+            e = launch_unpack(io.dtype, in.buf[0], in.W, in.H, in.D, in.P, io.out, st);
+            if (e != cudaSuccess) rc = cuda_fail(e, "unpack");
+        }
+    }
+    cudaFreeHost(h_flag);
+    b->stats_valid = true;
+    b->last_mode = 1;
+    return rc;
+}
+
+extern "C" int bgt_batch_run(bgt_batch *b, int mode, int use_graph)
+{
+    if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    cudaSetDevice(b->ctx->device);
+    int rc = mode == 1 ? run_plain(b) : run_engine(b, use_graph);
+    if (rc != BGT_OK) return rc;
+    return BGT_OK;
+}
+
+// Synchronise and turn the kernels' status word into an error code.
+int bgt::batch_check(bgt_batch *b)
+{
+    cudaError_t e = cudaStreamSynchronize(b->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch run");
+    int status = 0;
+    e = cudaMemcpy(&status, &b->d_sched->status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "status readback");
+    if (status & (kErrTmaTimeout | kErrQueueTimeout | kErrQueueFull))
+        return fail(BGT_ERR_TIMEOUT, "device wait gave up (status bits 0x%x)", status);
+    if (status & kErrPassLimit) return fail(BGT_ERR_LIMIT, "an instance hit the pass cap");
+    return BGT_OK;
+}
+
+extern "C" int bgt_batch_instance_stats(bgt_batch *b, int id, int *passes, int *converged, int *cfg)
+{
+    if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    if (id < 0 || id >= (int)b->items.size()) return fail(BGT_ERR_ARG, "bad instance id");
+    if (!b->stats_valid) {
+        int rc = batch_check(b);
+        if (rc != BGT_OK) return rc;
+        std::vector<Inst> tmp(b->items.size());
+        cudaError_t e = cudaMemcpy(tmp.data(), b->d_insts, tmp.size() * sizeof(Inst), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "stats readback");
+        for (size_t i = 0; i < tmp.size(); i++) {
+            b->stats[i].passes = tmp[i].passes_run;
+            b->stats[i].converged = tmp[i].converged;
+        }
+        b->stats_valid = true;
+    }
+    if (passes) *passes = b->stats[id].passes;
+    if (converged) *converged = b->stats[id].converged;
+    if (cfg) *cfg = b->items[id].cfg;
+    return BGT_OK;
+}
+
+extern "C" int bgt_batch_device_bytes(bgt_batch *b, size_t *bytes)
+{
+    if (!b || !bytes) return fail(BGT_ERR_ARG, "null argument");
+    *bytes = b->pool_bytes;
+    return BGT_OK;
+}
+
+extern "C" int bgt_cfg_list(int dims, int *ids, int cap, int *n)
+{
+    int m = 0;
+    const int *l = dims == 3 ? cfg_ids_3d(&m) : cfg_ids_2d(&m);
+    if (n) *n = m;
+    for (int i = 0; i < m && i < cap && ids; i++) ids[i] = l[i];
+    return BGT_OK;
+}
+
+extern "C" int bgt_cfg_describe(int id, int *dims, int *k, int *tw, int *th, int *tz, int *smem_bytes)
+{
+    const CfgInfo *c = cfg_info(id);
+    if (!c) return fail(BGT_ERR_ARG, "unknown configuration %d", id);
+    if (dims) *dims = c->dims;
+    if (k) *k = c->k;
+    if (tw) *tw = c->TW;
+    if (th) *th = c->TH;
+    if (tz) *tz = c->TZc;
+    if (smem_bytes) *smem_bytes = c->smem;
+    return BGT_OK;
+}
+
+// ------------------------------------------------------------ drop-in -----
+// One cached single-instance batch per (dims, shape).
+int bgt::single_batch(bgt_ctx *c, int dims, int W, int H, int D, bgt_batch **out)
+{
+    auto key = std::make_tuple(dims, W, H, D);
+    auto it = c->cache.find(key);
+    if (it != c->cache.end()) {
+        *out = it->second;
+        return BGT_OK;
+    }
+    if (c->cache.size() >= 16) {  // bound resident memory: drop the oldest shapes
+        cudaStreamSynchronize(c->stream);
+        for (auto &kv : c->cache) bgt_batch_destroy(kv.second);
+        c->cache.clear();
+    }
+    bgt_batch *b = nullptr;
+    int rc = bgt_batch_create(c, &b);
+    if (rc == BGT_OK) rc = dims == 2 ? bgt_batch_add2d(b, W, H, -1, nullptr) : bgt_batch_add3d(b, W, H, D, -1, nullptr);
+    if (rc == BGT_OK) rc = bgt_batch_finalize(b);
+    if (rc != BGT_OK) {
+        bgt_batch_destroy(b);
+        return rc;
+    }
+    c->cache[key] = b;
+    *out = b;
+    return BGT_OK;
+}
+
+static int thin_device(bgt_ctx *c, int dims, int dtype, const void *d_in, int W, int H, int D, void *d_out)
+{
+    if (!c) return fail(BGT_ERR_ARG, "null context");
+    if (!d_in || !d_out) return fail(BGT_ERR_ARG, "null buffer");
+    if (dtype_size(dtype) == 0) return fail(BGT_ERR_ARG, "bad dtype %d", dtype);
+    cudaSetDevice(c->device);
+    bgt_batch *b = nullptr;
+    int rc = single_batch(c, dims, W, H, D, &b);
+    if (rc != BGT_OK) return rc;
+    rc = bgt_batch_set_io(b, 0, dtype, d_in, d_out);
+    if (rc == BGT_OK) rc = bgt_batch_run(b, 0, 0);
+    return rc;
+}
+
+extern "C" int bgt_thin2d_device(bgt_ctx *c, int dtype, const void *d_in, int w, int h, void *d_out)
+{
+    return thin_device(c, 2, dtype, d_in, w, h, 1, d_out);
+}
+
+extern "C" int bgt_thin3d_device(bgt_ctx *c, int dtype, const void *d_in, int w, int h, int d, void *d_out)
+{
+    return thin_device(c, 3, dtype, d_in, w, h, d, d_out);
+}
+
+static int thin_host(bgt_ctx *c, int dims, int dtype, const void *in, int W, int H, int D, void *out)
+{
+    if (!c) return fail(BGT_ERR_ARG, "null context");
+    if (!in || !out) return fail(BGT_ERR_ARG, "null buffer");
+    const size_t es = dtype_size(dtype);
+    if (es == 0) return fail(BGT_ERR_ARG, "bad dtype %d", dtype);
+    if (W < 1 || H < 1 || D < 1) return fail(BGT_ERR_ARG, "bad size %dx%dx%d", W, H, D);
+    cudaSetDevice(c->device);
+    const size_t bytes = es * (size_t)W * H * D;
+    void *d_io = nullptr;
+    int rc = ctx_scratch(c, 0, bytes, &d_io);
+    if (rc != BGT_OK) return rc;
+    cudaError_t e = cudaMemcpyAsync(d_io, in, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "H2D");
+    bgt_batch *b = nullptr;
+    rc = single_batch(c, dims, W, H, D, &b);
+    if (rc != BGT_OK) return rc;
+    rc = bgt_batch_set_io(b, 0, dtype, d_io, d_io);  // unpack after the engine: in place is safe
+    if (rc == BGT_OK) rc = bgt_batch_run(b, 0, 0);
+    if (rc != BGT_OK) return rc;
+    e = cudaMemcpyAsync(out, d_io, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "D2H");
+    return batch_check(b);
+}
+
+extern "C" int bgt_thin2d(bgt_ctx *c, int dtype, const void *in, int w, int h, void *out)
+{
+    return thin_host(c, 2, dtype, in, w, h, 1, out);
+}
+
+extern "C" int bgt_thin3d(bgt_ctx *c, int dtype, const void *in, int w, int h, int d, void *out)
+{
+    return thin_host(c, 3, dtype, in, w, h, d, out);
+}
+
+extern "C" void bgt_free(void *p) { free(p); }

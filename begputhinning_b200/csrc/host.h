@@ -1,0 +1,92 @@
+// host.h -- host-side structures behind the C ABI handles.
+#pragma once
+#include <cstddef>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "bgt_capi.h"
+#include "common.cuh"
+
+struct bgt_batch;
+
+namespace bgt {
+struct Sched;
+
+struct Scratch {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct BatchItem {
+    int dims = 2, W = 0, H = 0, D = 1, cfg = -1;
+};
+
+struct IO {
+    int dtype = 0;
+    const void *in = nullptr;
+    void *out = nullptr;
+    int inW = 0, inH = 0, inD = 0;  // input extents (0: the instance's own)
+};
+
+struct Stat {
+    int passes = 0, converged = 0;
+};
+
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+size_t dtype_size(int dtype);
+int default_cfg(int dims, int W, int H, int D);
+int tuned_cfg(int dims, int W, int H, int D);
+int ctx_scratch(bgt_ctx *c, int slot, size_t bytes, void **out);
+int single_batch(bgt_ctx *c, int dims, int W, int H, int D, bgt_batch **out);
+int batch_check(bgt_batch *b);
+int batch_set_input_extent(bgt_batch *b, int id, int inW, int inH, int inD);
+
+// Segment list on the host (malloc'ed arrays), in the reference's emission order.
+struct HostSegs {
+    int nseg = 0, npts = 0;
+    int32_t *start = nullptr;
+    uint8_t *is_end = nullptr;
+    int16_t *px = nullptr, *py = nullptr, *pz = nullptr;
+};
+// Device ExtractSegmentsV on a packed image (P words per row).
+int segments_packed(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, int D, int P, HostSegs *out);
+void free_host_segs(HostSegs *s);
+}  // namespace bgt
+
+struct bgt_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::vector<bgt::Scratch> scratch;
+    std::map<std::tuple<int, int, int, int>, bgt_batch *> cache;
+};
+
+struct bgt_batch {
+    bgt_ctx *ctx = nullptr;
+    std::vector<bgt::BatchItem> items;
+    std::vector<bgt::Inst> h;
+    std::vector<bgt::IO> io;
+    std::vector<bgt::Stat> stats;
+    bool finalized = false;
+    bool stats_valid = false;
+    int last_mode = 0;
+    void *pool = nullptr;
+    size_t pool_bytes = 0;
+    bgt::Sched *d_sched = nullptr;
+    unsigned *d_seq = nullptr;
+    int4 *d_item = nullptr;
+    bgt::Inst *d_insts = nullptr;
+    CUtensorMap *d_tmaps = nullptr;
+    int *d_flag = nullptr;
+    unsigned cap = 0;
+    int smem = 0;
+    int grid = 0;
+    cudaGraphExec_t gexec = nullptr;
+    bool graph_valid = false;
+};

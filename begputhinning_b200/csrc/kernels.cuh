@@ -1,0 +1,53 @@
+// kernels.cuh -- declarations shared by the kernel translation unit and the
+// host-side batch/engine code.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace bgt {
+
+// Tile configurations.  2D ids 0..7: (K, S) with NW = 4 warps; 3D ids 16..18:
+// (NWX = 4, TZ).  All use 128 threads so the persistent engine can run any
+// mix of them in one launch.
+struct CfgInfo {
+    int id, dims, k, S, NW, NWX, TZ;
+    int TW, TH, TZc;  // core tile extent (words, rows, planes)
+    int smem;         // dynamic shared memory bytes
+    int box[3];       // TMA box (words, rows, planes)
+};
+const CfgInfo *cfg_info(int id);  // nullptr if unknown
+const int *cfg_ids_2d(int *n);
+const int *cfg_ids_3d(int *n);
+
+// Scheduler state of the persistent engine (device memory).
+struct Sched {
+    unsigned head;      // next ticket to consume
+    unsigned tail;      // next ticket to produce
+    int live;           // instances not yet converged
+    int status;         // error bits
+    unsigned cap;       // ring slots
+    unsigned pad[3];
+    unsigned *seq;      // [cap] slot sequence numbers
+    int4 *item;         // [cap] (instance, tile, pass, 0)
+    long long timeout_ns;
+};
+
+// Launchers (stream-ordered, no host synchronisation).
+// mode 0: 2D binarisation, 1: 3D binarisation, 2: nonzero.  Input extents
+// inW x inH x inD (row stride inW) inside the packed W x H x D.
+cudaError_t launch_pack(int dtype, int mode, const void *in, int inW, int inH, int inD, int W, int H, int D, int P,
+                        uint32_t *buf0, uint32_t *buf1, cudaStream_t st);
+cudaError_t launch_unpack(int dtype, const uint32_t *buf, int W, int H, int D, int P, void *out,
+                          cudaStream_t st);
+// per-tile nonempty marks -> lc (-1 nonempty, kNever empty); counts nonempty tiles into *count
+cudaError_t launch_tile_init(const Inst *d_inst, const Inst &h_inst, int *d_count, cudaStream_t st);
+cudaError_t launch_plain_pass(int cfg, Inst *d_inst, int ntiles, int q, int *d_flag, int *d_err,
+                              cudaStream_t st);
+cudaError_t launch_engine(int grid, int smem, Inst *d_insts, int ninst, Sched *d_sched, cudaStream_t st);
+int engine_max_blocks_per_sm(int smem);
+cudaError_t engine_set_smem(int smem);
+
+}  // namespace bgt

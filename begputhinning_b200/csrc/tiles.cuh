@@ -1,0 +1,282 @@
+// tiles.cuh -- the per-tile pass bodies shared by the plain (one launch per
+// pass) driver and the persistent batched engine.
+//
+// 2D tile, configuration (K, S, NW): a CTA of NW warps.  Warp w owns 32
+// consecutive rows, one row per lane; the lane holds S+2 words of its row in
+// registers (S core words plus one halo word each side).  K subiterations run
+// on those registers: y-neighbours come from the lanes above/below through
+// warp shuffles, x-neighbours from the adjacent registers through funnel
+// shifts.  Lanes 0..K-1 and 32-K..31 are halo rows (their state is only
+// valid for the lanes inside them), so a warp keeps 32-2K core rows and
+// consecutive warps overlap by 2K rows.  The tile (core plus halo) is staged
+// into shared memory by one TMA load; out-of-image parts read as zero.
+//
+// 3D tile, configuration (NWX, TZ): one subiteration per pass.  Warp w owns
+// word column x0+w; its lanes are 32 consecutive rows (30 core rows and one
+// halo row each side).  The warp marches through TZ+2 planes keeping a
+// 3-plane window of 3x3 (row, word) neighbourhoods in registers: three
+// shared-memory loads per plane, y-neighbours by shuffles, x-neighbours by
+// funnel shifts.  Mode 0 evaluates all six directional rules (the pre-test
+// union of the iteration, stored per word) and applies U; modes 1..5 apply
+// N, E, D, S, W masked by the stored union.
+#pragma once
+#include "common.cuh"
+#include "rules.cuh"
+
+namespace bgt {
+
+// ---------------------------------------------------------------- 2D ------
+template <int S, int DIR>
+__device__ __forceinline__ void subit2d(uint32_t (&v)[S + 2], uint32_t &chg)
+{
+    uint32_t prev_old = 0, up_prev = 0, dn_prev = 0;
+    uint32_t old_j = v[0];
+    uint32_t up_j = __shfl_up_sync(kFull, old_j, 1);
+    uint32_t dn_j = __shfl_down_sync(kFull, old_j, 1);
+#pragma unroll
+    for (int j = 0; j < S + 2; j++) {
+        uint32_t old_n = 0, up_n = 0, dn_n = 0;
+        if (j + 1 < S + 2) {
+            old_n = v[j + 1];
+            up_n = __shfl_up_sync(kFull, old_n, 1);
+            dn_n = __shfl_down_sync(kFull, old_n, 1);
+        }
+        uint32_t X[8];
+        X[0] = up_j;
+        X[1] = at_xp1(up_j, up_n);
+        X[2] = at_xp1(old_j, old_n);
+        X[3] = at_xp1(dn_j, dn_n);
+        X[4] = dn_j;
+        X[5] = at_xm1(dn_j, dn_prev);
+        X[6] = at_xm1(old_j, prev_old);
+        X[7] = at_xm1(up_j, up_prev);
+        const uint32_t del = old_j & rule2d<DIR>(X);
+        v[j] = old_j ^ del;
+        if (j >= 1 && j <= S) chg |= del;
+        prev_old = old_j;
+        up_prev = up_j;
+        dn_prev = dn_j;
+        old_j = old_n;
+        up_j = up_n;
+        dn_j = dn_n;
+    }
+}
+
+template <int K, int S, int PH, int I = 0>
+__device__ __forceinline__ void run_subits2d(uint32_t (&v)[S + 2], uint32_t &chg)
+{
+    if constexpr (I < K) {
+        subit2d<S, (PH + I) & 3>(v, chg);
+        run_subits2d<K, S, PH, I + 1>(v, chg);
+    }
+}
+
+template <int K, int S, int NW>
+struct Cfg2D {
+    static constexpr int kK = K, kS = S, kNW = NW;
+    static constexpr int CORE = 32 - 2 * K;   // core rows per warp
+    static constexpr int TH = NW * CORE;      // core rows per tile
+    static constexpr int BW = S + 8;          // box width in words (x0-4 .. x0+S+4)
+    static constexpr int BH = TH + 2 * K;     // box height in rows
+    static constexpr int SMEM = BW * BH * 4;  // bytes
+    static constexpr int THREADS = NW * 32;
+    static_assert(S % 4 == 0, "S must be a multiple of 4 (TMA x alignment, 128-bit stores)");
+    static_assert(BW <= 256 && BH <= 256, "TMA box too large");
+};
+
+// Process one 2D tile for pass q (phase PH = first direction of the pass).
+// Returns (to all threads) whether any core pixel was deleted.
+template <class C, int PH>
+__device__ bool tile2d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar, uint32_t &parity,
+                       int *err)
+{
+    constexpr int K = C::kK, S = C::kS, CORE = C::CORE, BW = C::BW, BH = C::BH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = tile % in.tiles_x, ty = tile / in.tiles_x;
+    const int x0 = tx * S, y0 = ty * C::TH;
+    const CUtensorMap *tm = in.tmap + (q & 1);
+    uint32_t *dst = in.buf[(q + 1) & 1];
+
+    if (threadIdx.x == 0) {
+        tmap_acquire(tm);
+        mbar_arrive_expect_tx(bar, (uint32_t)C::SMEM);
+        tma_load_2d(smem, tm, x0 - 4, y0 - K, bar);
+    }
+    if (!mbar_wait_bounded(bar, parity)) {
+        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
+    }
+    parity ^= 1u;
+
+    const int r = warp * CORE + lane;  // box row of this lane
+    const uint32_t *row = smem + r * BW;
+    uint32_t v[S + 2];
+    v[0] = row[3];
+#pragma unroll
+    for (int c = 0; c < S / 4; c++) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(row + 4 + 4 * c);
+        v[1 + 4 * c] = t.x;
+        v[2 + 4 * c] = t.y;
+        v[3 + 4 * c] = t.z;
+        v[4 + 4 * c] = t.w;
+    }
+    v[S + 1] = row[S + 4];
+
+    uint32_t chg = 0;
+    run_subits2d<K, S, PH>(v, chg);
+
+    const int y = y0 + r - K;  // image row of this lane
+    const bool core = lane >= K && lane < 32 - K && y < in.H;
+    if (core) {
+        uint32_t *drow = dst + (size_t)y * in.P + x0;
+#pragma unroll
+        for (int c = 0; c < S / 4; c++)
+            if (x0 + 4 * c < in.P)
+                *reinterpret_cast<uint4 *>(drow + 4 * c) =
+                    make_uint4(v[1 + 4 * c], v[2 + 4 * c], v[3 + 4 * c], v[4 + 4 * c]);
+        __threadfence();
+    }
+    const bool any = __syncthreads_or(core && chg != 0);  // also frees smem for the next tile
+    (void)BH;
+    return any;
+}
+
+// ---------------------------------------------------------------- 3D ------
+template <int NWX, int TZ>
+struct Cfg3D {
+    static constexpr int kNWX = NWX, kTZ = TZ;
+    static constexpr int TY = 30;             // core rows per tile (lanes 1..30)
+    static constexpr int BW = NWX + 8;        // box width in words
+    static constexpr int BH = 32;             // box rows
+    static constexpr int BD = TZ + 2;         // box planes
+    static constexpr int SMEM = BW * BH * BD * 4;
+    static constexpr int THREADS = NWX * 32;
+    static_assert(NWX % 4 == 0, "NWX must be a multiple of 4 (TMA x alignment)");
+    static_assert(BD <= 256, "TMA box too large");
+};
+
+__device__ __forceinline__ void plane3x3(const uint32_t *p, int col, uint32_t (&o)[9])
+{
+    const uint32_t l = p[col - 1], c = p[col], r = p[col + 1];
+    const uint32_t lu = __shfl_up_sync(kFull, l, 1), cu = __shfl_up_sync(kFull, c, 1),
+                   ru = __shfl_up_sync(kFull, r, 1);
+    const uint32_t ld = __shfl_down_sync(kFull, l, 1), cd = __shfl_down_sync(kFull, c, 1),
+                   rd = __shfl_down_sync(kFull, r, 1);
+    o[0] = at_xm1(cu, lu); o[1] = cu; o[2] = at_xp1(cu, ru);
+    o[3] = at_xm1(c, l);   o[4] = c;  o[5] = at_xp1(c, r);
+    o[6] = at_xm1(cd, ld); o[7] = cd; o[8] = at_xp1(cd, rd);
+}
+
+// MODE 0: pre-test union (stored) + U.  MODE 1..5: N, E, D, S, W.
+template <class C, int MODE>
+__device__ bool tile3d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar, uint32_t &parity,
+                       int *err)
+{
+    constexpr int NWX = C::kNWX, TZ = C::kTZ, BW = C::BW, BH = C::BH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = tile % in.tiles_x;
+    const int ty = (tile / in.tiles_x) % in.tiles_y;
+    const int tz = tile / (in.tiles_x * in.tiles_y);
+    const int x0 = tx * NWX, y0 = ty * C::TY, z0 = tz * TZ;
+    const CUtensorMap *tm = in.tmap + (q & 1);
+    uint32_t *dst = in.buf[(q + 1) & 1];
+
+    if (threadIdx.x == 0) {
+        tmap_acquire(tm);
+        mbar_arrive_expect_tx(bar, (uint32_t)C::SMEM);
+        tma_load_3d(smem, tm, x0 - 4, y0 - 1, z0 - 1, bar);
+    }
+    if (!mbar_wait_bounded(bar, parity)) {
+        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
+    }
+    parity ^= 1u;
+
+    const int col = 4 + warp;
+    const int x = x0 + warp, y = y0 + lane - 1;
+    const int wwords = (in.W + 31) >> 5;
+    const bool lane_live = lane >= 1 && lane <= 30 && y < in.H && x < wwords;
+    const size_t plane_words = (size_t)in.P * in.H;
+    const size_t base = (size_t)y * in.P + x;
+
+    uint32_t A[9], B[9], Cn[9];
+    plane3x3(smem + (0 * BH + lane) * BW, col, A);
+    plane3x3(smem + (1 * BH + lane) * BW, col, B);
+    uint32_t chg = 0;
+#pragma unroll 1
+    for (int zz = 0; zz < TZ; zz++) {
+        plane3x3(smem + ((zz + 2) * BH + lane) * BW, col, Cn);
+        const int z = z0 + zz;
+        const bool live = lane_live && z < in.D;
+        const uint32_t val = B[4];
+        uint32_t nv = val;
+        if (__any_sync(kFull, live && val != 0u)) {
+            uint32_t g[27];
+#pragma unroll
+            for (int i = 0; i < 9; i++) {
+                g[i] = A[i];
+                g[9 + i] = B[i];
+                g[18 + i] = Cn[i];
+            }
+            const size_t idx = (size_t)z * plane_words + base;
+            uint32_t del;
+            if constexpr (MODE == 0) {
+                const uint32_t du = rule3d<0>(g);
+                const uint32_t un = du | rule3d<1>(g) | rule3d<2>(g) | rule3d<3>(g) | rule3d<4>(g) | rule3d<5>(g);
+                if (live) in.uni[idx] = un & val;
+                del = val & du;
+            } else {
+                const uint32_t un = live ? ld_cg(in.uni + idx) : 0u;
+                del = val & rule3d<MODE>(g) & un;
+            }
+            nv = val & ~del;
+            if (live) chg |= del;
+        }
+        if (live) dst[(size_t)z * plane_words + base] = nv;
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+            A[i] = B[i];
+            B[i] = Cn[i];
+        }
+    }
+    (void)NWX;
+    __threadfence();
+    return __syncthreads_or(chg != 0u);
+}
+
+// ------------------------------------------------------------ activity ----
+// A tile may skip pass q when no tile of its 3x3(x3) neighbourhood changed
+// during the last `window` passes: its neighbourhood has then been constant
+// long enough to be a local fixed point for every direction.  Empty tiles
+// (lc == kNever) never change.
+__device__ __forceinline__ int nbr_last_change(const Inst &in, int tile)
+{
+    const int tx = tile % in.tiles_x;
+    const int ty = (tile / in.tiles_x) % in.tiles_y;
+    const int tz = tile / (in.tiles_x * in.tiles_y);
+    int m = kNever;
+    for (int dz = -1; dz <= 1; dz++) {
+        const int z = tz + dz;
+        if (z < 0 || z >= in.tiles_z) continue;
+        for (int dy = -1; dy <= 1; dy++) {
+            const int yy = ty + dy;
+            if (yy < 0 || yy >= in.tiles_y) continue;
+            for (int dx = -1; dx <= 1; dx++) {
+                const int xx = tx + dx;
+                if (xx < 0 || xx >= in.tiles_x) continue;
+                m = max(m, ld_cg_int(in.lc + (z * in.tiles_y + yy) * in.tiles_x + xx));
+            }
+        }
+    }
+    return m;
+}
+
+__device__ __forceinline__ bool tile_active(const Inst &in, int tile, int q)
+{
+    if (ld_cg_int(in.lc + tile) == kNever) return false;
+    if (in.dims == 2) return nbr_last_change(in, tile) >= q - in.window;
+    // 3D: decided at the first pass of an iteration (the union pass) for the
+    // whole iteration; a tile inactive there has an empty union and cannot
+    // change until the next iteration.
+    return nbr_last_change(in, tile) >= q - 6;
+}
+
+}  // namespace bgt

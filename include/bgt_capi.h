@@ -1,0 +1,141 @@
+/*
+ * bgt_capi.h -- C ABI of the B200 thinning library (libbgt.so).
+ *
+ * Plain C types only: host or device pointers, sizes, integer status codes.
+ * Every entry point returns BGT_OK (0) or a positive bgt_status; the message
+ * of the last failure on the calling thread is available from
+ * bgt_last_error().  Nothing here exits the process or reads stdin.
+ *
+ * Pixel data is row-major with x fastest: 2D data[y*width + x],
+ * 3D data[(z*height + y)*width + x].  Foreground follows the reference's
+ * binarisation: 2D (unsigned int)v > 0 (2D/CUDA_DeviceHelperFunctions.cuh:101),
+ * 3D int(v) > 0 (3D/CenterlineExtraction.cpp:44).  Thinned outputs are 0/1 in
+ * the input's pixel type.
+ */
+#ifndef BGT_CAPI_H
+#define BGT_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Pixel types of the reference's explicit instantiations
+ * (2D/LibThinning2D.cu:134-143, 2D/CenterlineExtraction.cpp:146-155). */
+typedef enum bgt_dtype {
+    BGT_U8 = 0,   /* unsigned char */
+    BGT_I8 = 1,   /* signed char */
+    BGT_CHAR = 2, /* char */
+    BGT_U16 = 3,  /* unsigned short */
+    BGT_I16 = 4,  /* short */
+    BGT_U32 = 5,  /* unsigned int */
+    BGT_I32 = 6,  /* int */
+    BGT_F32 = 7,  /* float */
+    BGT_F64 = 8,  /* double */
+    BGT_BOOL = 9  /* bool (one byte) */
+} bgt_dtype;
+
+typedef enum bgt_status {
+    BGT_OK = 0,
+    BGT_ERR_ARG = 1,      /* invalid argument (null pointer, bad size or dtype) */
+    BGT_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+    BGT_ERR_NOMEM = 3,    /* device or host allocation failed */
+    BGT_ERR_TIMEOUT = 4,  /* a bounded device wait gave up (status word set by a kernel) */
+    BGT_ERR_LIMIT = 5,    /* an instance hit the pass cap or a size limit */
+    BGT_ERR_STATE = 6     /* call out of order (e.g. run before finalize) */
+} bgt_status;
+
+typedef struct bgt_ctx bgt_ctx;     /* device, stream, resident scratch */
+typedef struct bgt_batch bgt_batch; /* a set of images/volumes thinned together */
+
+/* ---- context ---------------------------------------------------------- */
+/* Binds `device`; creates a private stream.  Resident device scratch grows on
+ * demand and is kept until bgt_ctx_destroy. */
+int bgt_ctx_create(int device, bgt_ctx **out);
+int bgt_ctx_destroy(bgt_ctx *ctx);
+/* Use a caller stream (cudaStream_t passed as void*) for subsequent calls;
+ * NULL restores the context's own stream. */
+int bgt_ctx_set_stream(bgt_ctx *ctx, void *stream);
+const char *bgt_last_error(void);
+int bgt_version(void);
+
+/* ---- drop-in thinning (host buffers, synchronous) ---------------------
+ * Replace Thinning2D<T> (2D/LibThinning2D.h:14-15) and Thinning3D<T>
+ * (3D/LibThinning3D.h:14-15): `in` and `out` are host arrays of `dtype`
+ * with width*height(*depth) elements; any size >= 1 is accepted. */
+int bgt_thin2d(bgt_ctx *ctx, int dtype, const void *in, int width, int height, void *out);
+int bgt_thin3d(bgt_ctx *ctx, int dtype, const void *in, int width, int height, int depth, void *out);
+
+/* ---- device-resident thinning (device buffers, stream-ordered) -------- */
+int bgt_thin2d_device(bgt_ctx *ctx, int dtype, const void *d_in, int width, int height, void *d_out);
+int bgt_thin3d_device(bgt_ctx *ctx, int dtype, const void *d_in, int width, int height, int depth,
+                      void *d_out);
+
+/* ---- centreline extraction (host buffers, synchronous) ----------------
+ * Replace CenterlineExtraction<T> (2D/CenterlineExtraction.h:25-28,
+ * 3D/CenterlineExctraction.h:26-29): thinning, segment extraction, pruning
+ * of end segments with at most max_segment_length points, moving-average
+ * smoothing with half-width smoothing_span, CSR output.  *out_x, *out_y
+ * (*out_z), *out_idx are allocated with malloc (free with bgt_free);
+ * out_idx has nsegs+1 entries, out_idx[nsegs] = number of points. */
+int bgt_centerline2d(bgt_ctx *ctx, int dtype, const void *in, int width, int height, int max_segment_length,
+                     int smoothing_span, float **out_x, float **out_y, unsigned int **out_idx,
+                     unsigned int *nsegs);
+int bgt_centerline3d(bgt_ctx *ctx, int dtype, const void *in, int width, int height, int depth,
+                     int max_segment_length, int smoothing_span, float **out_x, float **out_y, float **out_z,
+                     unsigned int **out_idx, unsigned int *nsegs);
+void bgt_free(void *p);
+
+/* ---- segment extraction on the device -------------------------------
+ * Replace ExtractSegmentsV<T> (2D/ExtractSegments.h:16-17,
+ * 3D/ExtractSegments.h:21-22) on a thinned 0/1 image already in device
+ * memory.  Outputs (host, malloc'ed, free with bgt_free): per segment its
+ * start offset (nseg+1 entries) and is_end_segment flag; per point x, y (z)
+ * as int16.  Segments come in the reference's emission order. */
+int bgt_segments2d_device(bgt_ctx *ctx, int dtype, const void *d_img, int width, int height, int32_t **start,
+                          uint8_t **is_end, int16_t **px, int16_t **py, int *nseg, int *npts);
+int bgt_segments3d_device(bgt_ctx *ctx, int dtype, const void *d_vol, int width, int height, int depth,
+                          int32_t **start, uint8_t **is_end, int16_t **px, int16_t **py, int16_t **pz, int *nseg,
+                          int *npts);
+
+/* ---- batched thinning ---------------------------------------------------
+ * Hundreds of images/volumes of uneven size thinned together by one
+ * persistent launch fed by a device-side queue of (instance, tile) work
+ * items, each instance converging on its own.  Usage: create, add shapes,
+ * finalize (allocates, picks tile configurations), set device input/output
+ * pointers, run (any number of times), destroy. */
+int bgt_batch_create(bgt_ctx *ctx, bgt_batch **out);
+int bgt_batch_destroy(bgt_batch *b);
+/* cfg < 0 lets the autotuner choose; returns the instance id in *id */
+int bgt_batch_add2d(bgt_batch *b, int width, int height, int cfg, int *id);
+int bgt_batch_add3d(bgt_batch *b, int width, int height, int depth, int cfg, int *id);
+int bgt_batch_finalize(bgt_batch *b);
+int bgt_batch_set_io(bgt_batch *b, int id, int dtype, const void *d_in, void *d_out);
+/* mode 0: persistent engine (optionally replayed as a CUDA graph when
+ * use_graph != 0); mode 1: plain path, one launch per pass per instance with
+ * a host readback of the change flag after every pass. */
+int bgt_batch_run(bgt_batch *b, int mode, int use_graph);
+/* per-instance passes run and whether it converged (1) / hit the cap (-1) */
+int bgt_batch_instance_stats(bgt_batch *b, int id, int *passes, int *converged, int *cfg);
+/* device bytes held by the batch */
+int bgt_batch_device_bytes(bgt_batch *b, size_t *bytes);
+
+/* ---- tile configurations and the autotuner's table --------------------
+ * The autotuner (begputhinning_b200/tune.py) times the configurations on
+ * sample instances of each size class and records the winner here; batches
+ * finalized afterwards use it for instances added with cfg < 0. */
+int bgt_tune_class(int dims, int width, int height, int depth);
+int bgt_tune_set(int dims, int cls, int cfg); /* cfg < 0 restores the default */
+int bgt_tune_get(int dims, int cls, int *cfg);
+
+/* Number of configurations for dims (2 or 3) and their ids. */
+int bgt_cfg_list(int dims, int *ids, int cap, int *n);
+/* k = subiterations per pass, tw/th/tz = core tile extent (words, rows, planes) */
+int bgt_cfg_describe(int id, int *dims, int *k, int *tw, int *th, int *tz, int *smem_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

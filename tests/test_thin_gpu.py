@@ -1,0 +1,167 @@
+"""GPU parity of the thinning kernels against the oracle (bit-exact).
+
+Every call goes through libbgt.so's C ABI (ctypes).  The oracle is the CPU
+restatement in oracle/ (itself pinned against the reference's own code in
+tests/test_oracle.py)."""
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from tests.helpers import blobs2d, blobs3d, random2d, random3d
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases2d(seed=0):
+    rng = np.random.default_rng(seed)
+    cases = [
+        np.zeros((1, 1), np.uint8), np.ones((1, 1), np.uint8), np.ones((3, 3), np.uint8),
+        np.zeros((40, 70), np.uint8), np.ones((1, 100), np.uint8), np.ones((100, 1), np.uint8),
+        np.ones((17, 33), np.uint8), np.ones((64, 64), np.uint8),
+    ]
+    for h, w in [(5, 5), (31, 33), (64, 96), (97, 131), (200, 300), (130, 1030)]:
+        cases.append(random2d(rng, h, w, 0.5))
+        cases.append(random2d(rng, h, w, 0.9))
+        cases.append(blobs2d(rng, h, w, max(1, h * w // 800)))
+    return cases
+
+
+def _cases3d(seed=1):
+    rng = np.random.default_rng(seed)
+    cases = [np.zeros((1, 1, 1), np.uint8), np.ones((3, 3, 3), np.uint8), np.ones((5, 7, 9), np.uint8)]
+    for d, h, w in [(6, 7, 9), (20, 33, 35), (40, 40, 70), (33, 64, 65)]:
+        cases.append(random3d(rng, d, h, w, 0.5))
+        cases.append(blobs3d(rng, d, h, w, max(1, d * h * w // 3000)))
+    return cases
+
+
+def _run_batch(ctx, imgs, cfg, plain):
+    import torch
+    from begputhinning_b200 import Batch
+    b = Batch(ctx)
+    ids = [b.add(im.shape, cfg) for im in imgs]
+    b.finalize()
+    ins = [torch.from_numpy(im).cuda() for im in imgs]
+    outs = [torch.empty_like(t) for t in ins]
+    for i, t, o in zip(ids, ins, outs):
+        b.set_io(i, t, o)
+    b.run(plain=plain)
+    torch.cuda.synchronize()
+    res = [o.cpu().numpy() for o in outs]
+    stats = [b.stats(i) for i in ids]
+    b.close()
+    return res, stats
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_thin2d_all_cfgs(ctx, plain):
+    from begputhinning_b200 import cfg_list
+    imgs = _cases2d()
+    want = [po.thin2d(im)[0] for im in imgs]
+    for cfg in cfg_list(2):
+        got, stats = _run_batch(ctx, imgs, cfg, plain)
+        for k, (g, w) in enumerate(zip(got, want)):
+            assert np.array_equal(g, w), f"cfg {cfg} case {k} shape {imgs[k].shape}: {(g != w).sum()} px differ"
+        assert all(s["converged"] == 1 for s in stats), (cfg, stats)
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_thin3d_all_cfgs(ctx, plain):
+    from begputhinning_b200 import cfg_list
+    vols = _cases3d()
+    want = [po.thin3d(v)[0] for v in vols]
+    for cfg in cfg_list(3):
+        got, stats = _run_batch(ctx, vols, cfg, plain)
+        for k, (g, w) in enumerate(zip(got, want)):
+            assert np.array_equal(g, w), f"cfg {cfg} case {k} shape {vols[k].shape}: {(g != w).sum()} vx differ"
+        assert all(s["converged"] == 1 for s in stats), (cfg, stats)
+
+
+def test_mixed_batch_engine(ctx):
+    """2D and 3D instances of uneven size in one persistent launch, default configs."""
+    rng = np.random.default_rng(7)
+    items = []
+    for i in range(24):
+        if i % 3 == 2:
+            items.append(blobs3d(rng, *rng.integers(8, 48, 3), 4))
+        else:
+            h, w = rng.integers(16, 400, 2)
+            items.append(blobs2d(rng, h, w, max(1, h * w // 1500)))
+    got, stats = _run_batch(ctx, items, -1, False)
+    for k, (g, it) in enumerate(zip(got, items)):
+        w = po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
+        assert np.array_equal(g, w), f"instance {k} shape {it.shape}"
+
+
+def test_engine_repeatable_and_graph(ctx):
+    """Replaying the captured graph gives the same result every time."""
+    import torch
+    from begputhinning_b200 import Batch
+    rng = np.random.default_rng(11)
+    imgs = [blobs2d(rng, 300, 260, 30), blobs3d(rng, 30, 40, 50, 5)]
+    want = [po.thin2d(imgs[0])[0], po.thin3d(imgs[1])[0]]
+    b = Batch(ctx)
+    ids = [b.add(im.shape) for im in imgs]
+    b.finalize()
+    ins = [torch.from_numpy(im).cuda() for im in imgs]
+    outs = [torch.zeros_like(t) for t in ins]
+    for i, t, o in zip(ids, ins, outs):
+        b.set_io(i, t, o)
+    for rep in range(3):
+        for o in outs:
+            o.zero_()
+        b.run(graph=True)
+        torch.cuda.synchronize()
+        for o, w in zip(outs, want):
+            assert np.array_equal(o.cpu().numpy(), w), f"replay {rep}"
+    b.close()
+
+
+DTYPES = [np.uint8, np.int8, np.uint16, np.int16, np.uint32, np.int32, np.float32, np.float64, np.bool_]
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_thin_dtypes_host_api(ctx, dt):
+    """Thinning2D / Thinning3D on every pixel type, with the reference's
+    binarisation (2D: (unsigned)v > 0 on the device; 3D: int(v) > 0)."""
+    from begputhinning_b200 import Thinning2D, Thinning3D
+    from begputhinning_b200.api import dtype_code
+    rng = np.random.default_rng(3)
+    base = blobs2d(rng, 70, 90, 8)
+    vals = np.array([0, 1, 2, -1, 0.5, 1.5, -3.7, 300, 70000], dtype=np.float64)
+    noise = rng.integers(0, len(vals), base.shape)
+    raw = np.where(base > 0, vals[noise], 0)
+    if dt == np.bool_:
+        a = raw != 0
+    else:
+        with np.errstate(all="ignore"):
+            a = raw.astype(dt)
+    fg = po.binarise(a, dtype_code(a.dtype), 2)
+    out = Thinning2D(a, ctx)
+    assert out.dtype == a.dtype
+    assert np.array_equal(out.astype(np.uint8) != 0, po.thin2d(fg)[0] != 0)
+    v3 = np.stack([a] * 6)[:, :40, :50].copy()
+    fg3 = po.binarise(v3, dtype_code(v3.dtype), 3)
+    out3 = Thinning3D(v3, ctx)
+    assert np.array_equal(out3.astype(np.uint8) != 0, po.thin3d(fg3)[0] != 0)
+
+
+def test_thin_device_api(ctx):
+    import torch
+    from begputhinning_b200 import thin_device
+    rng = np.random.default_rng(5)
+    img = blobs2d(rng, 257, 513, 40)
+    got = thin_device(torch.from_numpy(img).cuda(), ctx=ctx)
+    torch.cuda.synchronize()
+    assert np.array_equal(got.cpu().numpy(), po.thin2d(img)[0])
+
+
+def test_config_shapes_parity(ctx):
+    """Generator shapes at reduced size (frame strokes, vessels, trees)."""
+    from begputhinning_b200 import Thinning2D, Thinning3D, synth
+    img = synth.frame512(0)
+    assert np.array_equal(Thinning2D(img, ctx), po.thin2d(img)[0])
+    ves = synth.vessels2d(5, 1024, 768, nroots=6)
+    assert np.array_equal(Thinning2D(ves, ctx), po.thin2d(ves)[0])
+    vol = synth.trees3d(6, 96, 80, 72, ntrees=3, nell=1)
+    assert np.array_equal(Thinning3D(vol, ctx), po.thin3d(vol)[0])
