@@ -17,7 +17,7 @@ EXPORTS = [
     "bgt_centerline2d", "bgt_centerline3d", "bgt_free",
     "bgt_segments2d_device", "bgt_segments3d_device",
     "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
-    "bgt_batch_set_io", "bgt_batch_run", "bgt_batch_instance_stats", "bgt_batch_device_bytes",
+    "bgt_batch_set_io", "bgt_batch_run", "bgt_batch_instance_stats", "bgt_batch_device_bytes", "bgt_batch_work", "bgt_batch_stage_ms",
     "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe",
 ]
 
@@ -68,6 +68,8 @@ def _declare(L):
         "bgt_batch_run": [vp, I, I],
         "bgt_batch_instance_stats": [vp, I, ip, ip, ip],
         "bgt_batch_device_bytes": [vp, C.POINTER(C.c_size_t)],
+        "bgt_batch_work": [vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)],
+        "bgt_batch_stage_ms": [vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)],
         "bgt_tune_class": [I, I, I, I],
         "bgt_tune_set": [I, I, I],
         "bgt_tune_get": [I, I, ip],

@@ -274,6 +274,18 @@ class Batch:
         check(lib().bgt_batch_instance_stats(self.h, i, C.byref(p), C.byref(c), C.byref(g)))
         return {"passes": p.value, "converged": c.value, "cfg": g.value}
 
+    def work(self):
+        """(tiles processed, packed core words processed) of the last run."""
+        t, w = C.c_ulonglong(), C.c_ulonglong()
+        check(lib().bgt_batch_work(self.h, C.byref(t), C.byref(w)))
+        return t.value, w.value
+
+    def stage_ms(self):
+        """(pack, engine, unpack) device milliseconds of the last engine run."""
+        a, b, c = C.c_float(), C.c_float(), C.c_float()
+        check(lib().bgt_batch_stage_ms(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def device_bytes(self) -> int:
         n = C.c_size_t()
         check(lib().bgt_batch_device_bytes(self.h, C.byref(n)))

@@ -60,8 +60,23 @@ struct alignas(16) Inst {
     int converged;            // 1 when the instance reached its fixed point
     int passes_run;           // passes executed
     int pass_cap;             // safety cap on passes
-    long long tiles_run;      // tiles processed (skips excluded)
+    int prio;                 // work ring: 0 = critical path (served first), 1 = the rest
+    unsigned long long tiles_run;   // tiles processed (skipped tiles excluded)
+    unsigned long long work_words;  // packed core words processed (sum over passes and tiles)
 };
+
+// Core words of a tile (clamped to the image): the algorithmic unit of a pass.
+__device__ __forceinline__ unsigned tile_core_words(const Inst &in, int tile)
+{
+    const int wwords = (in.W + 31) >> 5;
+    const int tx = tile % in.tiles_x;
+    const int ty = (tile / in.tiles_x) % in.tiles_y;
+    const int tz = tile / (in.tiles_x * in.tiles_y);
+    const int cw = min(in.TW, wwords - tx * in.TW);
+    const int ch = min(in.TH, in.H - ty * in.TH);
+    const int cz = min(in.TZ, in.D - tz * in.TZ);
+    return (unsigned)(cw * ch * cz);
+}
 
 // ---------------------------------------------------------------------------
 // PTX wrappers: mbarrier + TMA (no cluster multicast anywhere in this code).

@@ -168,6 +168,11 @@ extern "C" int bgt_batch_create(bgt_ctx *ctx, bgt_batch **out)
 
 static void batch_free_device(bgt_batch *b)
 {
+    for (auto &ev : b->ev)
+        if (ev) {
+            cudaEventDestroy(ev);
+            ev = nullptr;
+        }
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;
     b->graph_valid = false;
@@ -252,22 +257,33 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
         const int maxdim = std::max(it.W, std::max(it.H, it.D));
         const int passes_per_iter = it.dims == 3 ? 6 : std::max(1, 4 / c.k);
         in.pass_cap = (maxdim + 16) * passes_per_iter + 64;
+        // 3D instances carry the longest chains of dependent passes (six
+        // passes per iteration): their waves go to the ring served first
+        in.prio = it.dims == 3 ? 0 : 1;
         const size_t words = (size_t)in.P * it.H * it.D;
         Offs &o = offs[i];
         o.b0 = off; off = align_up(off + words * 4, 256);
         o.b1 = off; off = align_up(off + words * 4, 256);
         if (it.dims == 3) { o.uni = off; off = align_up(off + words * 4, 256); }
-        o.lc = off; off = align_up(off + (size_t)in.ntiles * 4, 256);
         o.act = off; off = align_up(off + (size_t)in.ntiles, 256);
         o.list = off; off = align_up(off + (size_t)in.ntiles * 4, 256);
         total_tiles += in.ntiles;
         max_smem = std::max(max_smem, c.smem);
     }
+    // all per-tile "last change" arrays in one block (one memset per run)
+    const size_t off_lc = off;
+    for (int i = 0; i < N; i++) {
+        offs[i].lc = off;
+        off += (size_t)b->h[i].ntiles * 4;
+    }
+    b->lc_bytes = off - off_lc;
+    off = align_up(off, 256);
+    const size_t off_io = off; off = align_up(off + (size_t)N * sizeof(IODesc), 256);
     // scheduler + ring + instance table + tensor maps + flags
     const unsigned cap = (unsigned)(total_tiles + 1024);
     const size_t off_sched = off; off = align_up(off + sizeof(Sched), 256);
-    const size_t off_seq = off; off = align_up(off + (size_t)cap * 4, 256);
-    const size_t off_item = off; off = align_up(off + (size_t)cap * sizeof(int4), 256);
+    const size_t off_seq = off; off = align_up(off + (size_t)cap * 4 * 2, 256);
+    const size_t off_item = off; off = align_up(off + (size_t)cap * sizeof(int4) * 2, 256);
     const size_t off_inst = off; off = align_up(off + (size_t)N * sizeof(Inst), 256);
     const size_t off_tmap = off; off = align_up(off + (size_t)N * 2 * sizeof(CUtensorMap), 256);
     const size_t off_flag = off; off = align_up(off + 64, 256);
@@ -281,6 +297,8 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     b->d_insts = (Inst *)(P + off_inst);
     b->d_tmaps = (CUtensorMap *)(P + off_tmap);
     b->d_flag = (int *)(P + off_flag);
+    b->d_lc = P + off_lc;
+    b->d_io = (IODesc *)(P + off_io);
     b->cap = cap;
     std::vector<CUtensorMap> maps((size_t)N * 2);
     for (int i = 0; i < N; i++) {
@@ -316,9 +334,35 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     }
     const int per_sm = std::max(1, engine_max_blocks_per_sm(max_smem));
     b->grid = b->ctx->sms * per_sm;
+    for (auto &ev : b->ev) {
+        e = cudaEventCreate(&ev);
+        if (e != cudaSuccess) {
+            batch_free_device(b);
+            return cuda_fail(e, "cudaEventCreate");
+        }
+    }
     b->io.assign(N, IO());
     b->stats.assign(N, Stat());
     b->finalized = true;
+    return BGT_OK;
+}
+
+// Device time of the stages of the last engine run: pack (with the mark
+// reset and scheduler reset), engine (seed + persistent kernel), unpack.
+extern "C" int bgt_batch_stage_ms(bgt_batch *b, float *pack_ms, float *engine_ms, float *unpack_ms)
+{
+    if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    if (b->last_mode != 0) return fail(BGT_ERR_STATE, "stage times exist only for engine runs");
+    cudaError_t e = cudaEventSynchronize(b->ev[3]);
+    if (e != cudaSuccess) return cuda_fail(e, "event sync");
+    float t[3] = {0, 0, 0};
+    for (int k = 0; k < 3; k++) {
+        e = cudaEventElapsedTime(&t[k], b->ev[k], b->ev[k + 1]);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
+    }
+    if (pack_ms) *pack_ms = t[0];
+    if (engine_ms) *engine_ms = t[1];
+    if (unpack_ms) *unpack_ms = t[2];
     return BGT_OK;
 }
 
@@ -328,7 +372,10 @@ extern "C" int bgt_batch_set_io(bgt_batch *b, int id, int dtype, const void *d_i
     if (id < 0 || id >= (int)b->items.size()) return fail(BGT_ERR_ARG, "bad instance id %d", id);
     if (dtype_size(dtype) == 0) return fail(BGT_ERR_ARG, "bad dtype %d", dtype);
     IO &io = b->io[id];
-    if (io.in != d_in || io.out != d_out || io.dtype != dtype) b->graph_valid = false;
+    if (io.in != d_in || io.out != d_out || io.dtype != dtype) {
+        b->graph_valid = false;
+        b->io_dirty = true;
+    }
     io.dtype = dtype;
     io.in = d_in;
     io.out = d_out;
@@ -341,62 +388,114 @@ int bgt::batch_set_input_extent(bgt_batch *b, int id, int inW, int inH, int inD)
     const Inst &in = b->h[id];
     if (inW > in.W || inH > in.H || inD > in.D) return fail(BGT_ERR_ARG, "input extent larger than the instance");
     IO &io = b->io[id];
-    if (io.inW != inW || io.inH != inH || io.inD != inD) b->graph_valid = false;
+    if (io.inW != inW || io.inH != inH || io.inD != inD) {
+        b->graph_valid = false;
+        b->io_dirty = true;
+    }
     io.inW = inW;
     io.inH = inH;
     io.inD = inD;
     return BGT_OK;
 }
 
+// Both rings use `cap` slots; ring r's arrays are seq + r*cap, item + r*cap.
 __global__ void sched_reset_kernel(Sched *S, unsigned *seq, int4 *item, unsigned cap, long long timeout_ns)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
-        S->head = 0;
-        S->tail = 0;
+        for (int r = 0; r < 2; r++) {
+            S->ring[r].head = 0;
+            S->ring[r].tail = 0;
+            S->ring[r].cap = cap;
+            S->ring[r].seq = seq + (size_t)r * cap;
+            S->ring[r].item = item + (size_t)r * cap;
+        }
         S->live = 0;
+        S->live_prio[0] = 0;
+        S->live_prio[1] = 0;
         S->status = 0;
-        S->cap = cap;
-        S->seq = seq;
-        S->item = item;
         S->timeout_ns = timeout_ns;
     }
-    for (unsigned s = i; s < cap; s += gridDim.x * blockDim.x) seq[s] = s;
+    for (unsigned s = i; s < cap; s += gridDim.x * blockDim.x) {
+        seq[s] = s;
+        seq[cap + s] = s;
+    }
 }
 
-// Stream-ordered sequence of the engine run (capturable).
-static int enqueue_engine(bgt_batch *b, cudaStream_t st)
+// Upload the per-instance I/O table used by the batch-wide pack/unpack
+// (synchronous; done before any capture).
+static int upload_io(bgt_batch *b)
+{
+    if (!b->io_dirty) return BGT_OK;
+    const int N = (int)b->items.size();
+    std::vector<IODesc> io(N);
+    long long w = 0, g = 0;
+    for (int i = 0; i < N; i++) {
+        const Inst &in = b->h[i];
+        const IO &s = b->io[i];
+        if (!s.in) return fail(BGT_ERR_STATE, "instance %d has no input", i);
+        io[i].in = s.in;
+        io[i].out = s.out;
+        io[i].dtype = s.dtype;
+        io[i].mode = in.dims == 2 ? 0 : 1;
+        io[i].inW = s.inW ? s.inW : in.W;
+        io[i].inH = s.inH ? s.inH : in.H;
+        io[i].inD = s.inD ? s.inD : in.D;
+        io[i].inst = i;
+        io[i].wbegin = w;
+        io[i].gbegin = g;
+        w += (long long)in.P * in.H * in.D;
+        g += (long long)((in.W + 31) / 32) * in.H * in.D;
+    }
+    b->pack_words = w;
+    b->unpack_words = g;
+    b->any_out = false;
+    for (int i = 0; i < N; i++) b->any_out |= b->io[i].out != nullptr;
+    cudaError_t e = cudaMemcpy(b->d_io, io.data(), (size_t)N * sizeof(IODesc), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "I/O table upload");
+    b->io_dirty = false;
+    return BGT_OK;
+}
+
+// Stream-ordered sequence of the engine run (capturable): mark reset, one
+// batch-wide pack (which also marks non-empty tiles), scheduler reset, seed
+// + persistent engine, one batch-wide unpack.
+// Stage boundary event: inside a capture it must become an event-record node
+// (cudaEventRecordExternal); outside a capture it is a plain record.
+static void stage_event(cudaEvent_t ev, cudaStream_t st, bool capturing)
+{
+    if (capturing)
+        cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
+    else
+        cudaEventRecord(ev, st);
+}
+
+static int enqueue_engine(bgt_batch *b, cudaStream_t st, bool capturing)
 {
     const int N = (int)b->items.size();
-    cudaError_t e;
-    for (int i = 0; i < N; i++) {
-        const Inst &in = b->h[i];
-        const IO &io = b->io[i];
-        if (!io.in) return fail(BGT_ERR_STATE, "instance %d has no input", i);
-        e = launch_pack(io.dtype, in.dims == 2 ? 0 : 1, io.in, io.inW ? io.inW : in.W, io.inH ? io.inH : in.H,
-                        io.inD ? io.inD : in.D, in.W, in.H, in.D, in.P, in.buf[0], in.buf[1], st);
-        if (e != cudaSuccess) return cuda_fail(e, "pack");
-        e = launch_tile_init(b->d_insts + i, in, nullptr, st);
-        if (e != cudaSuccess) return cuda_fail(e, "tile init");
-    }
+    stage_event(b->ev[0], st, capturing);
+    cudaError_t e = cudaMemsetAsync(b->d_lc, 0x80, b->lc_bytes, st);
+    if (e == cudaSuccess) e = launch_pack_all(b->d_insts, b->d_io, N, b->pack_words, st);
+    if (e != cudaSuccess) return cuda_fail(e, "pack");
     sched_reset_kernel<<<std::min<unsigned>(1024, (b->cap + 255) / 256), 256, 0, st>>>(
         b->d_sched, b->d_seq, b->d_item, b->cap, 20000000000LL);
+    stage_event(b->ev[1], st, capturing);
     e = launch_engine(b->grid, b->smem, b->d_insts, N, b->d_sched, st);
     if (e != cudaSuccess) return cuda_fail(e, "engine launch");
-    for (int i = 0; i < N; i++) {
-        const Inst &in = b->h[i];
-        const IO &io = b->io[i];
-        if (!io.out) continue;
-        e = launch_unpack(io.dtype, in.buf[0], in.W, in.H, in.D, in.P, io.out, st);
+    stage_event(b->ev[2], st, capturing);
+    if (b->any_out) {
+        e = launch_unpack_all(b->d_insts, b->d_io, N, b->unpack_words, st);
         if (e != cudaSuccess) return cuda_fail(e, "unpack");
     }
+    stage_event(b->ev[3], st, capturing);
     return BGT_OK;
 }
 
 static int run_engine(bgt_batch *b, int use_graph)
 {
     cudaStream_t st = b->ctx->stream;
-    int rc;
+    int rc = upload_io(b);
+    if (rc != BGT_OK) return rc;
     if (use_graph) {
         if (!b->graph_valid) {
             if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -404,7 +503,7 @@ static int run_engine(bgt_batch *b, int use_graph)
             cudaGraph_t g = nullptr;
             cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
             if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
-            rc = enqueue_engine(b, st);
+            rc = enqueue_engine(b, st, true);
             e = cudaStreamEndCapture(st, &g);
             if (rc != BGT_OK) {
                 if (g) cudaGraphDestroy(g);
@@ -419,7 +518,7 @@ static int run_engine(bgt_batch *b, int use_graph)
         cudaError_t e = cudaGraphLaunch(b->gexec, st);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
     } else {
-        rc = enqueue_engine(b, st);
+        rc = enqueue_engine(b, st, false);
         if (rc != BGT_OK) return rc;
     }
     b->stats_valid = false;
@@ -446,6 +545,8 @@ static int run_plain(bgt_batch *b)
         e = launch_pack(io.dtype, in.dims == 2 ? 0 : 1, io.in, io.inW ? io.inW : in.W, io.inH ? io.inH : in.H,
                         io.inD ? io.inD : in.D, in.W, in.H, in.D, in.P, in.buf[0], in.buf[1], st);
         if (e == cudaSuccess) e = launch_tile_init(b->d_insts + i, in, nullptr, st);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(&b->d_insts[i].tiles_run, 0, 2 * sizeof(unsigned long long), st);
         if (e != cudaSuccess) { rc = cuda_fail(e, "pack"); break; }
         int last_change = -1;  // tiles start "changed just before pass 0"
         int q = 0;
@@ -521,6 +622,24 @@ extern "C" int bgt_batch_instance_stats(bgt_batch *b, int id, int *passes, int *
     if (passes) *passes = b->stats[id].passes;
     if (converged) *converged = b->stats[id].converged;
     if (cfg) *cfg = b->items[id].cfg;
+    return BGT_OK;
+}
+
+extern "C" int bgt_batch_work(bgt_batch *b, unsigned long long *tiles, unsigned long long *words)
+{
+    if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    int rc = batch_check(b);
+    if (rc != BGT_OK) return rc;
+    std::vector<Inst> tmp(b->items.size());
+    cudaError_t e = cudaMemcpy(tmp.data(), b->d_insts, tmp.size() * sizeof(Inst), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "work readback");
+    unsigned long long t = 0, w = 0;
+    for (const Inst &in : tmp) {
+        t += in.tiles_run;
+        w += in.work_words;
+    }
+    if (tiles) *tiles = t;
+    if (words) *words = w;
     return BGT_OK;
 }
 

@@ -15,6 +15,7 @@ struct bgt_batch;
 
 namespace bgt {
 struct Sched;
+struct IODesc;
 
 struct Scratch {
     void *ptr = nullptr;
@@ -84,9 +85,16 @@ struct bgt_batch {
     bgt::Inst *d_insts = nullptr;
     CUtensorMap *d_tmaps = nullptr;
     int *d_flag = nullptr;
+    void *d_lc = nullptr;         // contiguous per-tile "last change" arrays
+    size_t lc_bytes = 0;
+    bgt::IODesc *d_io = nullptr;  // per-instance I/O table of the batch-wide pack/unpack
+    bool io_dirty = true;
+    bool any_out = false;
+    long long pack_words = 0, unpack_words = 0;
     unsigned cap = 0;
     int smem = 0;
     int grid = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // stage boundaries of an engine run
     cudaGraphExec_t gexec = nullptr;
     bool graph_valid = false;
 };

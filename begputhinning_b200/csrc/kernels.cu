@@ -225,6 +225,201 @@ cudaError_t launch_unpack(int dtype, const uint32_t *buf, int W, int H, int D, i
     BGT_DISPATCH_DTYPE(dtype, unpack_t, buf, W, H, D, P, out, st)
 }
 
+// ------------------------------------------------------- batch-wide -------
+// One launch packs (or unpacks) every instance of a batch: the global word
+// index is mapped to its instance by a binary search over io[].wbegin.
+
+// 32 one-byte pixels starting at p -> bit word.  MSB-of-byte gather:
+// bytes that test true become 0x80 after the compare; multiplying the MSB
+// mask by 0x00204081 moves bits 7, 15, 23, 31 to 28..31 without carries.
+__device__ __forceinline__ uint32_t bytes4_to_bits(uint32_t cmp)
+{
+    return ((cmp & 0x80808080u) * 0x00204081u) >> 28;
+}
+
+// `room` = bytes readable from p onward (>= 36 allows the aligned 4-byte
+// loads that cover p .. p+31 whatever p's alignment).
+template <typename T, int MODE>
+__device__ __forceinline__ uint32_t pack_word(const T *p, int n, long long room = 0)
+{
+    if constexpr (sizeof(T) == 1 && (MODE != 1 || std::is_unsigned<T>::value || std::is_same<T, bool>::value)) {
+        // one-byte types whose test is "nonzero" (2D rule and unsigned/bool 3D rule)
+        if (n == 32 && (reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
+            const uint4 a = *reinterpret_cast<const uint4 *>(p);
+            const uint4 b = *reinterpret_cast<const uint4 *>(p + 16);
+            const uint32_t c[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            uint32_t w = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) w |= bytes4_to_bits(__vcmpne4(c[k], 0u)) << (4 * k);
+            return w;
+        }
+        // misaligned row: nine aligned words (p-3 .. p+35 at most, all inside
+        // the input: room counts bytes from p to the end, a negative room
+        // marks a word within 3 bytes of the input start), realigned with
+        // funnel shifts
+        if (n == 32 && room >= 36) {
+            const uintptr_t pa = reinterpret_cast<uintptr_t>(p);
+            const uint32_t *a = reinterpret_cast<const uint32_t *>(pa & ~uintptr_t(3));
+            const unsigned s = (unsigned)(pa & 3u) * 8u;
+            uint32_t prev = __ldg(a);
+            uint32_t w = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const uint32_t next = __ldg(a + k + 1);
+                const uint32_t c = __funnelshift_r(prev, next, s);
+                w |= bytes4_to_bits(__vcmpne4(c, 0u)) << (4 * k);
+                prev = next;
+            }
+            return w;
+        }
+    }
+    uint32_t w = 0;
+    for (int b = 0; b < n; b++) {
+        const T v = p[b];
+        const bool f = MODE == 0 ? fg2<T>(v) : MODE == 1 ? fg3<T>(v) : (v != (T)0);
+        w |= (uint32_t)f << b;
+    }
+    return w;
+}
+
+template <typename T>
+__device__ __forceinline__ uint32_t pack_word_mode(const T *p, int n, int mode, long long room)
+{
+    return mode == 0 ? pack_word<T, 0>(p, n, room) : mode == 1 ? pack_word<T, 1>(p, n, room)
+                                                               : pack_word<T, 2>(p, n, room);
+}
+
+__device__ __forceinline__ int find_io(const IODesc *io, int n, long long g, bool unpack)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((unpack ? io[mid].gbegin : io[mid].wbegin) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__restrict__ io, int n,
+                                long long total)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const IODesc &d = io[find_io(io, n, g, false)];
+        const Inst &in = insts[d.inst];
+        const long long i = g - d.wbegin;
+        const long long row = i / in.P;
+        const int j = (int)(i - row * in.P);
+        const int y = (int)(row % in.H), z = (int)(row / in.H);
+        const int x0 = j * 32;
+        uint32_t w = 0;
+        if (x0 < d.inW && y < d.inH && z < d.inD) {
+            const long long off = ((long long)z * d.inH + y) * (long long)d.inW + x0;
+            const int cnt = min(32, d.inW - x0);
+            // elements from off to the end of the input; words that start in the
+            // first 3 bytes of an unaligned input are kept on the scalar path
+            const bool head_ok = off >= 4 || (reinterpret_cast<uintptr_t>(d.in) & 3u) == 0;
+            const long long room = head_ok ? (long long)d.inW * d.inH * d.inD - off : 0;
+            switch (d.dtype) {
+            case BGT_U8: w = pack_word_mode((const uint8_t *)d.in + off, cnt, d.mode, room); break;
+            case BGT_I8: w = pack_word_mode((const int8_t *)d.in + off, cnt, d.mode, room); break;
+            case BGT_CHAR: w = pack_word_mode((const char *)d.in + off, cnt, d.mode, room); break;
+            case BGT_U16: w = pack_word_mode((const uint16_t *)d.in + off, cnt, d.mode, room); break;
+            case BGT_I16: w = pack_word_mode((const int16_t *)d.in + off, cnt, d.mode, room); break;
+            case BGT_U32: w = pack_word_mode((const uint32_t *)d.in + off, cnt, d.mode, room); break;
+            case BGT_I32: w = pack_word_mode((const int32_t *)d.in + off, cnt, d.mode, room); break;
+            case BGT_F32: w = pack_word_mode((const float *)d.in + off, cnt, d.mode, room); break;
+            case BGT_F64: w = pack_word_mode((const double *)d.in + off, cnt, d.mode, room); break;
+            default: w = pack_word_mode((const bool *)d.in + off, cnt, d.mode, room); break;
+            }
+        }
+        in.buf[0][i] = w;
+        in.buf[1][i] = w;
+        if (w) {  // tile holds foreground: lc = -1 (pre-filled with kNever)
+            const int t = ((z / in.TZ) * in.tiles_y + y / in.TH) * in.tiles_x + j / in.TW;
+            in.lc[t] = -1;
+        }
+    }
+}
+
+// 4 bits -> 4 bytes of value 0/1 (bit k to byte k): the multiplier places bit
+// k at 8k and the mask drops the other partial products (all at distinct bits).
+__device__ __forceinline__ uint32_t bits4_to_bytes(uint32_t nib) { return (nib * 0x00204081u) & 0x01010101u; }
+
+template <typename T>
+__device__ __forceinline__ void unpack_word(uint32_t w, T *o, int n)
+{
+    if constexpr (sizeof(T) == 1) {
+        if (n == 32 && (reinterpret_cast<uintptr_t>(o) & 15u) == 0) {
+            uint32_t c[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) c[k] = bits4_to_bytes((w >> (4 * k)) & 15u);
+            *reinterpret_cast<uint4 *>(o) = make_uint4(c[0], c[1], c[2], c[3]);
+            *reinterpret_cast<uint4 *>(o + 16) = make_uint4(c[4], c[5], c[6], c[7]);
+            return;
+        }
+        if (n == 32) {
+            // misaligned: head bytes up to a 4-byte boundary, seven aligned
+            // words, tail bytes; exactly the 32 bytes of this word are written
+            const unsigned h = (unsigned)((4u - (reinterpret_cast<uintptr_t>(o) & 3u)) & 3u);
+            uint8_t *ob = reinterpret_cast<uint8_t *>(o);
+            for (unsigned b = 0; b < h; b++) ob[b] = (uint8_t)((w >> b) & 1u);
+            uint32_t *oa = reinterpret_cast<uint32_t *>(ob + h);
+            const uint64_t ww = (uint64_t)w >> h;
+#pragma unroll
+            for (int k = 0; k < 7; k++) oa[k] = bits4_to_bytes((uint32_t)(ww >> (4 * k)) & 15u);
+            const unsigned done = h + 28;
+            for (unsigned b = done; b < 32; b++) ob[b] = (uint8_t)((w >> b) & 1u);
+            return;
+        }
+    }
+    for (int b = 0; b < n; b++) o[b] = (T)((w >> b) & 1u);
+}
+
+__global__ void unpack_all_kernel(const Inst *__restrict__ insts, const IODesc *__restrict__ io, int n,
+                                  long long total)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const IODesc &d = io[find_io(io, n, g, true)];
+        if (!d.out) continue;
+        const Inst &in = insts[d.inst];
+        const int wwords = (in.W + 31) >> 5;
+        const long long i = g - d.gbegin;
+        const long long row = i / wwords;
+        const int j = (int)(i - row * wwords);
+        const uint32_t w = __ldcg(in.buf[0] + row * in.P + j);
+        const long long off = row * (long long)in.W + (long long)j * 32;
+        const int cnt = min(32, in.W - j * 32);
+        switch (d.dtype) {
+        case BGT_U8: unpack_word(w, (uint8_t *)d.out + off, cnt); break;
+        case BGT_I8: unpack_word(w, (int8_t *)d.out + off, cnt); break;
+        case BGT_CHAR: unpack_word(w, (char *)d.out + off, cnt); break;
+        case BGT_U16: unpack_word(w, (uint16_t *)d.out + off, cnt); break;
+        case BGT_I16: unpack_word(w, (int16_t *)d.out + off, cnt); break;
+        case BGT_U32: unpack_word(w, (uint32_t *)d.out + off, cnt); break;
+        case BGT_I32: unpack_word(w, (int32_t *)d.out + off, cnt); break;
+        case BGT_F32: unpack_word(w, (float *)d.out + off, cnt); break;
+        case BGT_F64: unpack_word(w, (double *)d.out + off, cnt); break;
+        default: unpack_word(w, (bool *)d.out + off, cnt); break;
+        }
+    }
+}
+
+cudaError_t launch_pack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words,
+                            cudaStream_t st)
+{
+    pack_all_kernel<<<grid_for(total_words, 256), 256, 0, st>>>(d_insts, d_io, n, total_words);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words,
+                              cudaStream_t st)
+{
+    unpack_all_kernel<<<grid_for(total_words, 256), 256, 0, st>>>(d_insts, d_io, n, total_words);
+    return cudaGetLastError();
+}
+
 // --------------------------------------------------------- tile marks -----
 // lc[t] = -1 for tiles whose core holds foreground (lc pre-filled with kNever).
 __global__ void tile_mark_kernel(const Inst *__restrict__ pin)
@@ -290,9 +485,13 @@ __global__ void __launch_bounds__(kThreads) plain_pass_kernel(Inst *pin, int q, 
     if (!active) return;
     uint32_t parity = 0;
     const bool ch = run_tile(in, q, tile, smem, &bar, parity, err);
-    if (threadIdx.x == 0 && ch) {
-        in.lc[tile] = q;
-        atomicExch(flag, 1);
+    if (threadIdx.x == 0) {
+        atomicAdd(&pin->tiles_run, 1ull);
+        atomicAdd(&pin->work_words, (unsigned long long)tile_core_words(in, tile));
+        if (ch) {
+            in.lc[tile] = q;
+            atomicExch(flag, 1);
+        }
     }
 }
 
@@ -311,9 +510,14 @@ cudaError_t launch_plain_pass(int cfg, Inst *d_inst, int ntiles, int q, int *d_f
 }
 
 // ------------------------------------------------------------- engine -----
-// Work ring: Vyukov-style bounded MPMC queue.  seq[s] == t   : slot free for
-// ticket t (producer may write); seq[s] == t+1 : item of ticket t ready;
-// the consumer of ticket t then sets seq[s] = t + cap.
+// Two work rings (0: critical-path instances first, 1: the rest), each a
+// bounded MPMC queue with per-slot sequence numbers:
+//   seq[s] == t    slot free for ticket t (the producer may write it)
+//   seq[s] == t+1  item of ticket t ready
+//   the consumer of ticket t then sets seq[s] = t + cap.
+// Producers reserve tickets with an atomic on `tail`; consumers claim one by
+// CAS on `head`, only when head < tail, so an idle CTA never commits to a
+// ring it would have to wait on.
 
 __device__ __forceinline__ unsigned ld_acq_u(const unsigned *p)
 {
@@ -325,53 +529,110 @@ __device__ __forceinline__ void st_rel_u(unsigned *p, unsigned v)
 {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned ld_volatile_u(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 
-// Publish n items (instance ii, tiles list[0..n), pass q); whole CTA calls.
-__device__ void produce(Sched *S, int ii, const int *list, int n, int q)
+// Publish n items (instance ii, tiles list[0..n), pass q) on the instance's
+// ring; item.w carries n so a consumer knows the wave size.  Whole CTA calls.
+__device__ void produce(Sched *S, int ii, int prio, const int *list, int n, int q)
 {
     __shared__ unsigned t0;
-    if (threadIdx.x == 0) t0 = atomicAdd(&S->tail, (unsigned)n);
+    Ring &R = S->ring[prio];
+    if (threadIdx.x == 0) t0 = atomicAdd(&R.tail, (unsigned)n);
     __syncthreads();
-    const unsigned cap = S->cap;
+    const unsigned cap = R.cap;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const unsigned t = t0 + (unsigned)i;
         const unsigned s = t % cap;
-        const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
-        bool ok = false;
-        for (int spin = 0;; spin++) {
-            if (ld_acq_u(S->seq + s) == t) { ok = true; break; }
-            if ((spin & 255) == 255 && globaltimer() > t_end) break;
-            __nanosleep(64);
+        bool ok = ld_acq_u(R.seq + s) == t;
+        if (!ok) {
+            const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
+            for (int spin = 0;; spin++) {
+                __nanosleep(64);
+                if (ld_acq_u(R.seq + s) == t) { ok = true; break; }
+                if ((spin & 255) == 255 && globaltimer() > t_end) break;
+            }
         }
         if (!ok) {
             atomicOr(&S->status, kErrQueueFull);
             continue;
         }
-        S->item[s] = make_int4(ii, __ldcg(list + i), q, 0);
-        st_rel_u(S->seq + s, t + 1);
+        R.item[s] = make_int4(ii, __ldcg(list + i), q, n);
+        st_rel_u(R.seq + s, t + 1);
     }
     __syncthreads();
 }
 
-// Build the active list for pass q1 of instance ii and publish it (or retire
-// the instance).  Whole CTA calls.  Returns nothing; updates S->live.
-__device__ void next_wave(Sched *S, Inst *insts, int ii, int q1)
+// Active tiles of pass q1 (tiles whose 3x3(x3) neighbourhood changed within
+// the window), marked by scattering from the changed tiles into a bitmap in
+// shared memory; falls back to gathering per tile when the instance has more
+// tiles than the bitmap holds.  Whole CTA calls; returns the count.
+__device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int scratch_words)
+{
+    __shared__ int cnt;
+    const int nt = in.ntiles;
+    const int nwords = (nt + 31) >> 5;
+    if (threadIdx.x == 0) cnt = 0;
+    const int thr = q1 - window;
+    if (2 * nwords <= scratch_words) {
+        uint32_t *act = scratch, *ne = scratch + nwords;
+        for (int i = threadIdx.x; i < 2 * nwords; i += blockDim.x) scratch[i] = 0;
+        __syncthreads();
+        const int tx = in.tiles_x, ty = in.tiles_y, tz = in.tiles_z;
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+            const int v = ld_cg_int(in.lc + t);
+            if (v == kNever) continue;
+            atomicOr(ne + (t >> 5), 1u << (t & 31));
+            if (v < thr) continue;
+            const int x = t % tx, y = (t / tx) % ty, z = t / (tx * ty);
+            for (int dz = -1; dz <= 1; dz++) {
+                const int zz = z + dz;
+                if (zz < 0 || zz >= tz) continue;
+                for (int dy = -1; dy <= 1; dy++) {
+                    const int yy = y + dy;
+                    if (yy < 0 || yy >= ty) continue;
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const int xx = x + dx;
+                        if (xx < 0 || xx >= tx) continue;
+                        const int u = (zz * ty + yy) * tx + xx;
+                        atomicOr(act + (u >> 5), 1u << (u & 31));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
+            uint32_t m = act[w] & ne[w];
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                in.list[atomicAdd(&cnt, 1)] = (w << 5) + b;
+            }
+        }
+    } else {
+        __syncthreads();
+        for (int t = threadIdx.x; t < nt; t += blockDim.x)
+            if (ld_cg_int(in.lc + t) != kNever && nbr_last_change(in, t) >= thr) in.list[atomicAdd(&cnt, 1)] = t;
+    }
+    __syncthreads();
+    return cnt;
+}
+
+// Build the active list for pass q1 of instance ii and publish it, or retire
+// the instance.  Whole CTA calls.  3D instances rebuild the list only at
+// iteration starts (the union pass decides activity for the iteration).
+__device__ void next_wave(Sched *S, Inst *insts, int ii, int q1, int nprev, uint32_t *scratch, int scratch_words)
 {
     Inst &in = insts[ii];
     __shared__ int cnt;
-    const bool recompute = in.dims == 2 || q1 % 6 == 0;
-    if (threadIdx.x == 0) cnt = recompute ? 0 : __ldcg(&in.nlist);
-    __syncthreads();
-    if (recompute) {
-        for (int t = threadIdx.x; t < in.ntiles; t += blockDim.x) {
-            if (tile_active(in, t, q1)) {
-                const int p = atomicAdd(&cnt, 1);
-                in.list[p] = t;
-            }
-        }
-    }
-    __syncthreads();
-    const int n = cnt;
+    int n;
+    if (in.dims == 2) n = build_list(in, q1, in.window, scratch, scratch_words);
+    else if (q1 % 6 == 0) n = build_list(in, q1, 6, scratch, scratch_words);
+    else n = nprev;
     if (threadIdx.x == 0) {
         in.passes_run = q1;
         bool retire = n == 0;
@@ -381,39 +642,76 @@ __device__ void next_wave(Sched *S, Inst *insts, int ii, int q1)
         }
         if (retire) {
             in.converged = n == 0 ? 1 : -1;
-            in.nlist = 0;
         } else {
             in.pass = q1;
-            in.nlist = n;
             in.done = 0;
         }
         __threadfence();
-        if (retire) atomicSub(&S->live, 1);
+        if (retire) {
+            atomicSub(&S->live_prio[in.prio], 1);
+            atomicSub(&S->live, 1);
+        }
         cnt = retire ? 0 : n;
     }
     __syncthreads();
-    if (cnt > 0) {
-        __threadfence();
-        produce(S, ii, in.list, cnt, q1);
-    }
+    const int m = cnt;
+    if (m > 0) produce(S, ii, in.prio, in.list, m, q1);
 }
 
-// One CTA per instance: first wave (pass 0) after the tile marks.
+// One CTA per instance: marks reset done by the pack; first wave (pass 0).
 __global__ void __launch_bounds__(kThreads) engine_seed_kernel(Inst *insts, int ninst, Sched *S)
 {
+    __shared__ uint32_t scratch[2048];
     for (int ii = blockIdx.x; ii < ninst; ii += gridDim.x) {
         if (threadIdx.x == 0) {
             insts[ii].converged = 0;
             insts[ii].passes_run = 0;
+            insts[ii].tiles_run = 0;
+            insts[ii].work_words = 0;
+            atomicAdd(&S->live_prio[insts[ii].prio], 1);
             atomicAdd(&S->live, 1);
         }
         __syncthreads();
-        next_wave(S, insts, ii, 0);
+        next_wave(S, insts, ii, 0, 0, scratch, 2048);
         __syncthreads();
     }
 }
 
-__global__ void __launch_bounds__(kThreads) engine_kernel(Inst *insts, Sched *S)
+// Take a ticket of ring R (one fetch-and-add, no retry loop) when the ring
+// looks non-empty.  Several CTAs may see the same last item, so a ticket can
+// run past the items produced so far; its holder then waits for the ring's
+// next item (see wait_ticket).
+__device__ __forceinline__ bool take_ticket(Ring &R, unsigned &t)
+{
+    const unsigned h = ld_volatile_u(&R.head);
+    const unsigned tl = ld_volatile_u(&R.tail);
+    if ((int)(tl - h) <= 0) return false;
+    t = atomicAdd(&R.head, 1u);
+    return true;
+}
+
+// Wait for the item of ticket t of ring r.  Returns 1 with the item, 0 when
+// the ticket can never be filled (every instance of that ring retired and t
+// is past the final tail: the ticket is abandoned), -1 on timeout.
+__device__ __forceinline__ int wait_ticket(Sched *S, int r, unsigned t, int4 &out, unsigned long long t_end)
+{
+    Ring &R = S->ring[r];
+    const unsigned s = t % R.cap;
+    for (int w = 0;; w++) {
+        if (ld_acq_u(R.seq + s) == t + 1) {
+            out = __ldcg(R.item + s);
+            st_rel_u(R.seq + s, t + R.cap);
+            return 1;
+        }
+        if ((w & 15) == 15) {
+            if (ld_acquire(&S->live_prio[r]) == 0 && (int)(t - ld_volatile_u(&R.tail)) >= 0) return 0;
+            if (globaltimer() > t_end) return -1;
+        }
+        if (w > 8) __nanosleep(w < 64 ? 32 : 256);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) engine_kernel(Inst *insts, Sched *S, int scratch_words)
 {
     extern __shared__ __align__(128) uint32_t smem_raw[];
     uint32_t *smem = align128(smem_raw);
@@ -428,29 +726,37 @@ __global__ void __launch_bounds__(kThreads) engine_kernel(Inst *insts, Sched *S)
     uint32_t parity = 0;
     for (;;) {
         if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(&S->head, 1u);
-            const unsigned s = t % S->cap;
             const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
             int g = 0;
             for (int spin = 0;; spin++) {
-                if (ld_acq_u(S->seq + s) == t + 1) {
-                    item = __ldcg(S->item + s);
-                    st_rel_u(S->seq + s, t + S->cap);
+                unsigned t;
+                int r = -1;
+                if (take_ticket(S->ring[0], t)) r = 0;
+                else if (take_ticket(S->ring[1], t)) r = 1;
+                if (r >= 0) {
+                    int4 it;
+                    const int w = wait_ticket(S, r, t, it, t_end);
+                    if (w < 0) {
+                        atomicOr(&S->status, kErrQueueTimeout);
+                        break;
+                    }
+                    if (w == 0) continue;  // abandoned: that ring is finished
+                    item = it;
                     g = 1;
                     break;
                 }
                 if (ld_acquire(&S->live) == 0) break;
-                if ((spin & 255) == 255 && globaltimer() > t_end) {
+                if ((spin & 63) == 63 && globaltimer() > t_end) {
                     atomicOr(&S->status, kErrQueueTimeout);
                     break;
                 }
-                __nanosleep(spin < 64 ? 32 : 256);
+                __nanosleep(spin < 32 ? 20 : 200);
             }
             got = g;
         }
         __syncthreads();
         if (!got) break;
-        const int ii = item.x, tile = item.y, q = item.z;
+        const int ii = item.x, tile = item.y, q = item.z, nwave = item.w;
         Inst &in = insts[ii];
         fence_proxy_async_global();
         const bool ch = run_tile(in, q, tile, smem, &bar, parity, &S->status);
@@ -458,12 +764,14 @@ __global__ void __launch_bounds__(kThreads) engine_kernel(Inst *insts, Sched *S)
             if (ch) in.lc[tile] = q;
             __threadfence();
             const int d = atomicAdd(&in.done, 1);
-            last = d == __ldcg(&in.nlist) - 1;
+            last = d == nwave - 1;
+            atomicAdd(&in.tiles_run, 1ull);
+            atomicAdd(&in.work_words, (unsigned long long)tile_core_words(in, tile));
         }
         __syncthreads();
         if (last) {
             __threadfence();
-            next_wave(S, insts, ii, q + 1);
+            next_wave(S, insts, ii, q + 1, nwave, smem, scratch_words);
         }
         __syncthreads();
     }
@@ -488,7 +796,7 @@ cudaError_t launch_engine(int grid, int smem, Inst *d_insts, int ninst, Sched *d
     engine_seed_kernel<<<std::min(ninst, 148 * 8), kThreads, 0, st>>>(d_insts, ninst, d_sched);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    engine_kernel<<<grid, kThreads, smem + 128, st>>>(d_insts, d_sched);
+    engine_kernel<<<grid, kThreads, smem + 128, st>>>(d_insts, d_sched, smem / 4);
     return cudaGetLastError();
 }
 

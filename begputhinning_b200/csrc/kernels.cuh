@@ -23,19 +23,39 @@ const int *cfg_ids_2d(int *n);
 const int *cfg_ids_3d(int *n);
 
 // Scheduler state of the persistent engine (device memory).
-struct Sched {
-    unsigned head;      // next ticket to consume
-    unsigned tail;      // next ticket to produce
-    int live;           // instances not yet converged
-    int status;         // error bits
-    unsigned cap;       // ring slots
-    unsigned pad[3];
+struct alignas(128) Ring {
+    unsigned head;      // next ticket to claim
+    unsigned pad0[31];  // head and tail on separate 128-byte lines
+    unsigned tail;      // next ticket to reserve
+    unsigned cap;       // slots
     unsigned *seq;      // [cap] slot sequence numbers
-    int4 *item;         // [cap] (instance, tile, pass, 0)
+    int4 *item;         // [cap] (instance, tile, pass, tiles in the wave)
+};
+
+struct Sched {
+    Ring ring[2];       // 0: critical-path instances, 1: the rest
+    int live;           // instances not yet converged
+    int live_prio[2];   // ... per ring (a ring with no live instance gets no more items)
+    int status;         // error bits
     long long timeout_ns;
 };
 
+// Per-instance input/output of a batch-wide pack/unpack launch.
+struct alignas(16) IODesc {
+    const void *in;
+    void *out;
+    int dtype, mode;         // pixel type; binarisation 0 = 2D rule, 1 = 3D rule, 2 = nonzero
+    int inW, inH, inD;       // input extents inside the instance
+    int inst;                // instance index
+    long long wbegin;        // first global packed-word index of the instance (pack)
+    long long gbegin;        // first global unpack-word index (rows x ceil(W/32))
+};
+
 // Launchers (stream-ordered, no host synchronisation).
+cudaError_t launch_pack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words,
+                            cudaStream_t st);
+cudaError_t launch_unpack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words,
+                              cudaStream_t st);
 // mode 0: 2D binarisation, 1: 3D binarisation, 2: nonzero.  Input extents
 // inW x inH x inD (row stride inW) inside the packed W x H x D.
 cudaError_t launch_pack(int dtype, int mode, const void *in, int inW, int inH, int inD, int W, int H, int D, int P,

@@ -133,7 +133,6 @@ __device__ bool tile2d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t
             if (x0 + 4 * c < in.P)
                 *reinterpret_cast<uint4 *>(drow + 4 * c) =
                     make_uint4(v[1 + 4 * c], v[2 + 4 * c], v[3 + 4 * c], v[4 + 4 * c]);
-        __threadfence();
     }
     const bool any = __syncthreads_or(core && chg != 0);  // also frees smem for the next tile
     (void)BH;
@@ -238,7 +237,8 @@ __device__ bool tile3d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t
         }
     }
     (void)NWX;
-    __threadfence();
+    // the barrier orders every thread's stores before thread 0's fence and
+    // release (engine) or the end of the launch (plain path)
     return __syncthreads_or(chg != 0u);
 }
 

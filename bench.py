@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""Throughput of batched directional-subiteration thinning on one node.
+
+Workload (per GPU): the mixed batch -- 512 2D images with sides log-uniform
+64..2048 px (aspect 0.5..2) of Bezier strokes, plus 32 3D volumes with sides
+log-uniform 64..192 of tubular trees -- uint8 {0,1}, seeded synthetic data.
+A step is one pass of the hot path over the whole batch: batch-wide pack of
+the uint8 inputs (resident in HBM) into bit-packed words, one persistent
+engine launch that thins every instance to its own fixed point, batch-wide
+unpack to uint8 outputs; replayed as one CUDA graph.  ``value`` is thinned
+Mvoxel/s (pixels count as voxels) over all ranks.
+
+Also reported: ``e2e`` (the same step with inputs copied from pinned host
+memory and outputs copied back inside the timed region), the plain path
+(one launch per pass per instance with a host readback of the change flag
+after every pass) on the same batch, the roofline of the engine kernel, the
+CPU baseline (the oracle's OpenMP thinning on this host's cores, on a bounded
+sample) and the SM clocks sampled during the timed region.
+
+``--impl reference`` times the reference's own thinning rules on the host
+cores (oracle/_ref: the reference's rule functions run globally by an OpenMP
+driver) on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank thins its own batch (seed offset by rank);
+no collective is on the data path (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "thinned Mvoxel/s batched vs plain, bit-exact, 1xB200; serving p99 latency"
+UNIT = "Mvoxel/s"
+WORKLOAD = ("mixed batch: 512 2D stroke images, sides log-uniform 64-2048 (aspect 0.5-2), "
+            "+ 32 3D tree volumes, sides log-uniform 64-192; uint8 {0,1}")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="bgt", choices=["bgt", "reference"])
+    p.add_argument("--seed", type=int, default=3)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    p.add_argument("--n2d", type=int, default=512, help="2D instances per GPU (smaller only for profiling)")
+    p.add_argument("--n3d", type=int, default=32, help="3D instances per GPU (smaller only for profiling)")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-serve", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.gpu_id:
+                cmd += ["-i", self.gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the engine kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "engine_kernel_mixed_batch.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip().split()[0])
+    except Exception:
+        pass
+    return None
+
+
+def workload(seed: int, n2d: int = 512, n3d: int = 32):
+    from begputhinning_b200 import synth
+    imgs, vols = synth.mixed_batch(seed, n2d, n3d)
+    return imgs + vols
+
+
+def cpu_baseline(items, budget_s: float) -> dict:
+    """The oracle's OpenMP thinning on this host, on the first instances of
+    the batch until the time budget is spent."""
+    from oracle import pyoracle as po
+    cores = host_cores()
+    t0 = time.perf_counter()
+    vox = 0
+    n = 0
+    for it in items:
+        if it.ndim == 2:
+            po.thin2d(it, cores)
+        else:
+            po.thin3d(it, cores)
+        vox += it.size
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": vox / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {n} of {len(items)} instances ({vox / 1e6:.1f} Mvoxel), oracle OpenMP thinning"}
+
+
+def run_bgt(args, rank, world, local):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import begputhinning_b200 as bgt
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    items = workload(args.seed + 1000 * rank, args.n2d, args.n3d)
+    sizes = [it.size for it in items]
+    units = int(sum(sizes))
+    total = sum(sizes)
+    offs = np.cumsum([0] + sizes)
+
+    # inputs resident in HBM (one allocation), outputs likewise
+    host_in = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    hv = host_in.numpy()
+    for it, o in zip(items, offs):
+        hv[o:o + it.size] = it.reshape(-1)
+    host_out = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    dev_in = host_in.to(dev)
+    dev_out = torch.empty_like(dev_in)
+
+    ctx = bgt.Context(local)
+    stream = torch.cuda.Stream(dev)
+    ctx.set_stream(stream)
+    b = bgt.Batch(ctx)
+    ids = [b.add(it.shape) for it in items]
+    b.finalize()
+    for i, it, o in zip(ids, items, offs):
+        b.set_io(i, dev_in[o:o + it.size], dev_out[o:o + it.size])
+    torch.cuda.synchronize()
+
+    def step():
+        b.run(graph=True, sync=False)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+
+    # bit-exactness spot check of a few instances against the oracle
+    from oracle import pyoracle as po
+    out_np = dev_out.cpu().numpy()
+    rng = np.random.default_rng(rank)
+    small = [k for k, it in enumerate(items) if it.size <= 300_000]
+    checked = 0
+    for k in rng.choice(small, size=min(6, len(small)), replace=False):
+        it = items[k]
+        want = po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
+        got = out_np[offs[k]:offs[k] + it.size].reshape(it.shape)
+        if not np.array_equal(got, want):
+            raise SystemExit(f"bench parity check failed on instance {k} shape {it.shape}")
+        checked += 1
+
+    gpu_uuid = None
+    try:
+        gpu_uuid = str(torch.cuda.get_device_properties(local).uuid)
+        if not gpu_uuid.startswith("GPU-"):
+            gpu_uuid = "GPU-" + gpu_uuid
+    except Exception:
+        gpu_uuid = None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(gpu_uuid)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+
+    # engine kernel alone: stage events recorded by the library on the same stream
+    eng_ms, pack_ms, unpack_ms = [], [], []
+    for _ in range(max(3, args.steps // 2)):
+        with torch.cuda.stream(stream):
+            step()
+        p, e, u = b.stage_ms()
+        eng_ms.append(e)
+        pack_ms.append(p)
+        unpack_ms.append(u)
+    tiles, words = b.work()
+
+    # end to end: pinned host -> device, thin, device -> pinned host
+    torch.cuda.synchronize()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, args.steps // 2)
+    with torch.cuda.stream(stream):
+        dev_in.copy_(host_in, non_blocking=True)
+        step()
+        host_out.copy_(dev_out, non_blocking=True)
+        h0.record(stream)
+        for _ in range(e2e_steps):
+            dev_in.copy_(host_in, non_blocking=True)
+            step()
+            host_out.copy_(dev_out, non_blocking=True)
+        h1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = h0.elapsed_time(h1) / e2e_steps
+    if not torch.equal(host_out, dev_out.cpu()):
+        raise SystemExit("e2e output mismatch")
+
+    # plain path on the same batch (one launch per pass, host readback per pass)
+    plain = None
+    if not args.no_plain:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run(plain=True, sync=True)
+        plain_s = time.perf_counter() - t0
+        if not torch.equal(dev_out.cpu(), host_out):
+            raise SystemExit("plain path output differs from the engine")
+        plain = {"value": units / plain_s / 1e6, "unit": UNIT, "ms_per_step": plain_s * 1e3,
+                 "what": "one launch per pass per instance, host readback of the change flag after each pass"}
+
+    # cross-rank aggregation: max time, summed units
+    t = torch.tensor([ms, e2e_ms, statistics.median(eng_ms)], device=dev, dtype=torch.float64)
+    u = torch.tensor([units], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    ms_max, e2e_max, eng_max = t.tolist()
+    units_all = u.item()
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    eng = statistics.median(eng_ms)
+    alg_bytes = words * 8.0  # one 4-byte read + one 4-byte write per packed core word per pass
+    achieved = alg_bytes / (eng * 1e-3) / 1e9
+    n2 = sum(1 for it in items if it.ndim == 2)
+    line = {
+        "metric": METRIC,
+        "value": units_all / (ms_max * 1e-3) / 1e6,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u32",
+        "data": "synthetic (seeded generators of the workload shapes; no public dataset)",
+        "config": {"workload": WORKLOAD, "instances_2d": n2, "instances_3d": len(items) - n2,
+                   "voxels_per_gpu": units, "input_bytes_per_gpu": total,
+                   "l2": "inputs larger than L2 (uint8 inputs and outputs of several hundred MB per step)",
+                   "step": "batch-wide pack + persistent engine + batch-wide unpack, one CUDA graph",
+                   "parallelism": f"instances per rank, {world} rank(s), no collective"},
+        "e2e": {"value": units_all / (e2e_max * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": total,
+                "d2h_bytes_per_step": total,
+                "path": "pinned host -> HBM copy, the batch C ABI run, HBM -> pinned host copy"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,
+                     "kernel": "engine_kernel", "launch_ms": eng,
+                     "algorithmic_bytes_per_launch": alg_bytes, "tile_passes": tiles},
+        "stage_ms": {"pack": statistics.median(pack_ms), "engine": eng, "unpack": statistics.median(unpack_ms)},
+        "gpu_launches": 5 * args.steps,
+        "parity_checked_instances": checked,
+        "clocks": clk,
+    }
+    if plain:
+        line["plain"] = plain
+        line["batched_over_plain"] = line["value"] / plain["value"]
+    if world == 1:
+        line["cpu_baseline"] = cpu_baseline(items, args.cpu_seconds)
+    b.close()
+    ctx.close()
+    return line
+
+
+def run_reference(args, rank, world):
+    """The reference's own thinning rules on the host cores (oracle/_ref)."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+    if rank != 0:
+        return None
+    items = workload(args.seed, args.n2d, args.n3d)
+    have_ref = po.have_ref("2d") and po.have_ref("3d")
+    kind = "reference" if have_ref else "port"
+    # a bounded sample: a fixed subset of the batch sized so that every step
+    # takes a few seconds (probe the speed on the first instances)
+    order = list(range(len(items)))
+    rng = np.random.default_rng(0)
+    rng.shuffle(order)
+
+    def thin(it):
+        if have_ref:
+            return po.ref_thin2d(it) if it.ndim == 2 else po.ref_thin3d(it)
+        return po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
+
+    t0 = time.perf_counter()
+    sample = []
+    for k in order:
+        thin(items[k])
+        sample.append(k)
+        if time.perf_counter() - t0 > 1.5:
+            break
+    budget = max(1.0, 150.0 / max(1, args.steps + args.warmup))  # seconds per step
+    rate = sum(items[k].size for k in sample) / (time.perf_counter() - t0)
+    target = rate * budget
+    sample, vox = [], 0
+    for k in order:
+        if vox >= target and sample:
+            break
+        sample.append(k)
+        vox += items[k].size
+    for _ in range(args.warmup):
+        for k in sample[:1]:
+            thin(items[k])
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for k in sample:
+            thin(items[k])
+        times.append(time.perf_counter() - t0)
+    mean = statistics.mean(times)
+    value = vox / mean / 1e6
+    cores = host_cores()
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generators of the workload shapes)",
+        "config": {"workload": WORKLOAD, "sample_instances": len(sample), "sample_voxels": vox},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{len(sample)} of {len(items)} instances ({vox / 1e6:.1f} Mvoxel) per step; "
+                                   + ("the reference's rule functions, global synchronous OpenMP driver"
+                                      if have_ref else "the oracle's OpenMP port")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    try:
+        line = run_bgt(args, rank, world, local)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

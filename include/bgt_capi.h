@@ -121,6 +121,13 @@ int bgt_batch_run(bgt_batch *b, int mode, int use_graph);
 int bgt_batch_instance_stats(bgt_batch *b, int id, int *passes, int *converged, int *cfg);
 /* device bytes held by the batch */
 int bgt_batch_device_bytes(bgt_batch *b, size_t *bytes);
+/* work of the last run, summed over instances: tiles processed (skipped
+ * tiles excluded) and packed core words processed (one read + one write of
+ * 4 bytes each is the algorithmic traffic of a word-pass) */
+int bgt_batch_work(bgt_batch *b, unsigned long long *tiles, unsigned long long *words);
+/* device milliseconds of the last engine run's stages (CUDA events on the
+ * batch's stream): pack, engine (the persistent thinning kernel), unpack */
+int bgt_batch_stage_ms(bgt_batch *b, float *pack_ms, float *engine_ms, float *unpack_ms);
 
 /* ---- tile configurations and the autotuner's table --------------------
  * The autotuner (begputhinning_b200/tune.py) times the configurations on

@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #define __device__
@@ -27,47 +28,70 @@ static inline int min(int a, unsigned int b) { return (unsigned int)a < b ? a : 
 #include "oracle.h"
 
 namespace {
-inline unsigned int word_at(const std::vector<uint8_t> &img, int w, int h, int y, int xs)
-{
-    unsigned int v = 0;
-    if (y < 0 || y >= h) return 0;
-    for (int b = 0; b < 32; b++) {
-        int x = xs + b;
-        if (x >= 0 && x < w && img[(size_t)y * w + x]) v |= 1u << b;
+// Rows packed 64 pixels per word with one zero guard word on each side and
+// one zero guard row above and below; window(row, xs) = the 32 pixels
+// xs .. xs+31 as a rule-function word.
+struct Packed {
+    int w, h, nw;
+    std::vector<uint64_t> v;
+    Packed(int w_, int h_) : w(w_), h(h_), nw((w_ + 63) / 64), v((size_t)((w_ + 63) / 64 + 2) * (h_ + 2), 0) {}
+    uint64_t *row(int y) { return v.data() + (size_t)(y + 1) * (nw + 2); }
+    const uint64_t *row(int y) const { return v.data() + (size_t)(y + 1) * (nw + 2); }
+    static unsigned int window(const uint64_t *r, int xs)
+    {
+        const int b = xs + 64, k = b >> 6, s = b & 63;
+        uint64_t lo = r[k] >> s;
+        if (s) lo |= r[k + 1] << (64 - s);
+        return (unsigned int)lo;
     }
-    return v;
-}
+    static void put30(uint64_t *r, int x0, uint64_t bits)  // 30 bits at pixel x0
+    {
+        const int b = x0 + 64, k = b >> 6, s = b & 63;
+        r[k] |= bits << s;
+        if (s > 34) r[k + 1] |= bits >> (64 - s);
+    }
+};
 }  // namespace
 
+// Global, synchronous host execution of the reference's rule functions; each
+// rule call evaluates a 32-pixel window and keeps its 30 inner pixels.
 template <typename PixelType>
 void Thinning2D(int width, int height, PixelType *data, PixelType *out)
 {
-    std::vector<uint8_t> cur((size_t)width * height), nxt;
-    for (size_t i = 0; i < cur.size(); i++) cur[i] = (unsigned int)data[i] > 0;
+    Packed cur(width, height), nxt(width, height);
+    for (int y = 0; y < height; y++)
+        for (int x = 0; x < width; x++)
+            if ((unsigned int)data[(size_t)y * width + x] > 0) cur.row(y)[1 + x / 64] |= 1ull << (x % 64);
     typedef int (*rule_t)(unsigned int, unsigned int, unsigned int &);
     rule_t rules[4] = {North, South, East, West};
+    const uint64_t m30 = (1ull << 30) - 1;
     for (;;) {
-        int changed = 0;
+        long long changed = 0;
         for (int s = 0; s < 4; s++) {
-            nxt = cur;
-            for (int y = 0; y < height; y++)
+            std::fill(nxt.v.begin(), nxt.v.end(), 0);
+#pragma omp parallel for reduction(+ : changed) schedule(static)
+            for (int y = 0; y < height; y++) {
+                const uint64_t *ru = cur.row(y - 1), *rc = cur.row(y), *rd = cur.row(y + 1);
+                uint64_t *ro = nxt.row(y);
                 for (int x0 = 0; x0 < width; x0 += 30) {
-                    unsigned int up = word_at(cur, width, height, y - 1, x0 - 1);
-                    unsigned int cp = word_at(cur, width, height, y, x0 - 1);
-                    unsigned int dn = word_at(cur, width, height, y + 1, x0 - 1);
+                    unsigned int up = Packed::window(ru, x0 - 1), cp = Packed::window(rc, x0 - 1);
+                    const unsigned int dn = Packed::window(rd, x0 - 1), before = cp;
                     rules[s](up, dn, cp);
-                    for (int b = 1; b <= 30 && x0 + b - 1 < width; b++) {
-                        uint8_t nv = (cp >> b) & 1;
-                        size_t i = (size_t)y * width + x0 + b - 1;
-                        if (nv != cur[i]) changed = 1;
-                        nxt[i] = nv;
-                    }
+                    uint64_t keep = (uint64_t)(cp >> 1) & m30;
+                    const int valid = width - x0 < 30 ? width - x0 : 30;
+                    keep &= (valid == 30) ? m30 : ((1ull << valid) - 1);
+                    changed += __builtin_popcountll(((uint64_t)(before >> 1) & m30 & ~keep) &
+                                                    ((valid == 30) ? m30 : ((1ull << valid) - 1)));
+                    Packed::put30(ro, x0, keep);
                 }
-            cur.swap(nxt);
+            }
+            std::swap(cur.v, nxt.v);
         }
         if (!changed) break;
     }
-    for (size_t i = 0; i < cur.size(); i++) out[i] = (PixelType)cur[i];
+    for (int y = 0; y < height; y++)
+        for (int x = 0; x < width; x++)
+            out[(size_t)y * width + x] = (PixelType)((cur.row(y)[1 + x / 64] >> (x % 64)) & 1);
 }
 
 template void Thinning2D<unsigned char>(int, int, unsigned char *, unsigned char *);

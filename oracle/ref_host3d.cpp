@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #define __device__
@@ -22,81 +23,110 @@
 #include "oracle.h"
 
 namespace {
-struct Vol {
-    int w, h, d;
-    std::vector<uint8_t> v;
-    unsigned int word(int z, int y, int xs) const
-    {
-        if (z < 0 || z >= d || y < 0 || y >= h) return 0;
-        unsigned int r = 0;
-        for (int b = 0; b < 32; b++) {
-            int x = xs + b;
-            if (x >= 0 && x < w && v[((size_t)z * h + y) * w + x]) r |= 1u << b;
-        }
-        return r;
-    }
-};
 typedef unsigned int (*rule_t)(unsigned int, unsigned int *, unsigned int);
 const rule_t kOrder[6] = {Up3D, North3D, East3D, Down3D, South3D, West3D};
 
-// n[] for the word whose bit b is voxel x0-1+b (valid for bits 1..30)
-void gather(const Vol &V, int z, int y, int x0, unsigned int n[26], unsigned int &val)
+// Volume packed 64 voxels per word along x, with zero guard words/rows/planes.
+struct Packed3 {
+    int w, h, d, nw;
+    std::vector<uint64_t> v;
+    Packed3(int w_, int h_, int d_)
+        : w(w_), h(h_), d(d_), nw((w_ + 63) / 64), v((size_t)((w_ + 63) / 64 + 2) * (h_ + 2) * (d_ + 2), 0)
+    {
+    }
+    uint64_t *row(int z, int y) { return v.data() + ((size_t)(z + 1) * (h + 2) + (y + 1)) * (nw + 2); }
+    const uint64_t *row(int z, int y) const
+    {
+        return v.data() + ((size_t)(z + 1) * (h + 2) + (y + 1)) * (nw + 2);
+    }
+    static unsigned int window(const uint64_t *r, int xs)
+    {
+        const int b = xs + 64, k = b >> 6, s = b & 63;
+        uint64_t lo = r[k] >> s;
+        if (s) lo |= r[k + 1] << (64 - s);
+        return (unsigned int)lo;
+    }
+    static void put30(uint64_t *r, int x0, uint64_t bits)
+    {
+        const int b = x0 + 64, k = b >> 6, s = b & 63;
+        r[k] |= bits << s;
+        if (s > 34) r[k + 1] |= bits >> (64 - s);
+    }
+};
+
+// n[] in the reference's neighbour order for the window starting at xs
+inline void gather(const Packed3 &V, int z, int y, int xs, unsigned int n[26], unsigned int &val)
 {
     int i = 0;
     for (int dz = -1; dz <= 1; dz++)
-        for (int dy = -1; dy <= 1; dy++)
+        for (int dy = -1; dy <= 1; dy++) {
+            const uint64_t *r = V.row(z + dz, y + dy);
             for (int dx = -1; dx <= 1; dx++) {
-                unsigned int wv = V.word(z + dz, y + dy, x0 - 1 + dx);
+                const unsigned int wv = Packed3::window(r, xs + dx);
                 if (dz == 0 && dy == 0 && dx == 0) { val = wv; continue; }
                 n[i++] = wv;
             }
+        }
 }
 }  // namespace
 
+// Global, synchronous host execution of the reference's rule functions
+// (pre-test union on the iteration-start state, then U,N,E,D,S,W with that
+// mask as `prev`); each rule call keeps the 30 inner voxels of its window.
 template <typename PixelType>
 void Thinning3D(int width, int height, int depth, PixelType *data, PixelType *out)
 {
-    Vol cur{width, height, depth, std::vector<uint8_t>((size_t)width * height * depth)};
-    for (size_t i = 0; i < cur.v.size(); i++) cur.v[i] = data[i] > 0;
-    std::vector<unsigned int> pv;
+    Packed3 cur(width, height, depth), nxt(width, height, depth);
+    for (int z = 0; z < depth; z++)
+        for (int y = 0; y < height; y++)
+            for (int x = 0; x < width; x++)
+                if (data[((size_t)z * height + y) * width + x] > 0) cur.row(z, y)[1 + x / 64] |= 1ull << (x % 64);
+    const int nx = (width + 29) / 30;
+    std::vector<unsigned int> pv((size_t)nx * height * depth);
+    const uint64_t m30 = (1ull << 30) - 1;
+    const long long rows = (long long)depth * height;
     for (;;) {
-        int changed = 0;
-        // pre-test on the iteration-start state; one mask word per 30 voxels
-        const int nx = (width + 29) / 30;
-        pv.assign((size_t)nx * height * depth, 0);
-        for (int z = 0; z < depth; z++)
-            for (int y = 0; y < height; y++)
+        long long changed = 0;
+#pragma omp parallel for schedule(static)
+        for (long long zy = 0; zy < rows; zy++) {
+            const int z = (int)(zy / height), y = (int)(zy % height);
+            for (int c = 0; c < nx; c++) {
+                unsigned int n[26], val;
+                gather(cur, z, y, c * 30 - 1, n, val);
+                unsigned int p = Up3D(val, n);
+                p &= North3D(val, n);
+                p &= East3D(val, n);
+                p &= Down3D(val, n);
+                p &= South3D(val, n);
+                p &= West3D(val, n);
+                pv[(size_t)zy * nx + c] = p;
+            }
+        }
+        for (int s = 0; s < 6; s++) {
+            std::fill(nxt.v.begin(), nxt.v.end(), 0);
+#pragma omp parallel for reduction(+ : changed) schedule(static)
+            for (long long zy = 0; zy < rows; zy++) {
+                const int z = (int)(zy / height), y = (int)(zy % height);
+                uint64_t *ro = nxt.row(z, y);
                 for (int c = 0; c < nx; c++) {
                     unsigned int n[26], val;
-                    gather(cur, z, y, c * 30, n, val);
-                    unsigned int p = Up3D(val, n);
-                    p &= North3D(val, n);
-                    p &= East3D(val, n);
-                    p &= Down3D(val, n);
-                    p &= South3D(val, n);
-                    p &= West3D(val, n);
-                    pv[((size_t)z * height + y) * nx + c] = p;
+                    gather(cur, z, y, c * 30 - 1, n, val);
+                    const unsigned int r = kOrder[s](val, n, pv[(size_t)zy * nx + c]);
+                    const int valid = width - c * 30 < 30 ? width - c * 30 : 30;
+                    const uint64_t vm = valid == 30 ? m30 : ((1ull << valid) - 1);
+                    const uint64_t keep = (uint64_t)(r >> 1) & vm;
+                    changed += __builtin_popcountll((uint64_t)(val >> 1) & vm & ~keep);
+                    Packed3::put30(ro, c * 30, keep);
                 }
-        for (int s = 0; s < 6; s++) {
-            Vol nxt = cur;
-            for (int z = 0; z < depth; z++)
-                for (int y = 0; y < height; y++)
-                    for (int c = 0; c < nx; c++) {
-                        unsigned int n[26], val;
-                        gather(cur, z, y, c * 30, n, val);
-                        unsigned int r = kOrder[s](val, n, pv[((size_t)z * height + y) * nx + c]);
-                        for (int b = 1; b <= 30 && c * 30 + b - 1 < width; b++) {
-                            uint8_t nvb = (r >> b) & 1;
-                            size_t i = ((size_t)z * height + y) * width + c * 30 + b - 1;
-                            if (nvb != cur.v[i]) changed = 1;
-                            nxt.v[i] = nvb;
-                        }
-                    }
-            cur.v.swap(nxt.v);
+            }
+            std::swap(cur.v, nxt.v);
         }
         if (!changed) break;
     }
-    for (size_t i = 0; i < cur.v.size(); i++) out[i] = (PixelType)cur.v[i];
+    for (int z = 0; z < depth; z++)
+        for (int y = 0; y < height; y++)
+            for (int x = 0; x < width; x++)
+                out[((size_t)z * height + y) * width + x] = (PixelType)((cur.row(z, y)[1 + x / 64] >> (x % 64)) & 1);
 }
 
 template void Thinning3D<unsigned char>(int, int, int, unsigned char *, unsigned char *);
