@@ -13,7 +13,7 @@ SYNTH_PATH = os.path.join(PKG, "libbgt_synth.so")
 # names declared in include/bgt_capi.h (kept in sync by tests/test_capi_symbols.py)
 EXPORTS = [
     "bgt_ctx_create", "bgt_ctx_destroy", "bgt_ctx_set_stream", "bgt_last_error", "bgt_version",
-    "bgt_thin2d", "bgt_thin3d", "bgt_thin2d_device", "bgt_thin3d_device",
+    "bgt_thin2d", "bgt_thin3d", "bgt_thin2d_device", "bgt_thin3d_device", "bgt_thin2d_device_noalloc",
     "bgt_centerline2d", "bgt_centerline3d", "bgt_free",
     "bgt_segments2d_device", "bgt_segments3d_device",
     "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
@@ -51,6 +51,7 @@ def _declare(L):
         "bgt_thin3d": [vp, I, vp, I, I, I, vp],
         "bgt_thin2d_device": [vp, I, vp, I, I, vp],
         "bgt_thin3d_device": [vp, I, vp, I, I, I, vp],
+        "bgt_thin2d_device_noalloc": [I, I, vp, I, I, vp, vp],
         "bgt_centerline2d": [vp, I, vp, I, I, I, I, fpp, fpp, upp, up],
         "bgt_centerline3d": [vp, I, vp, I, I, I, I, I, fpp, fpp, fpp, upp, up],
         "bgt_segments2d_device": [vp, I, vp, I, I, C.POINTER(C.POINTER(C.c_int32)),

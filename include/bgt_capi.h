@@ -73,6 +73,24 @@ int bgt_thin2d_device(bgt_ctx *ctx, int dtype, const void *d_in, int width, int 
 int bgt_thin3d_device(bgt_ctx *ctx, int dtype, const void *d_in, int width, int height, int depth,
                       void *d_out);
 
+/* ---- thinning without device allocation --------------------------------
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory (a host application that owns all device memory through its
+ * own pool, a real-time loop that cannot afford an allocation's implicit
+ * synchronisation, work being recorded into a CUDA graph): thins one 2D
+ * image of `dtype` from d_in to d_out (device buffers, width*height pixels)
+ * on `stream` (a cudaStream_t, NULL = legacy default stream) of `device`,
+ * using only an 8 MiB scratch array compiled into the library (kept by
+ * every GPU that loads it until the process exits).  Images whose packed
+ * form does not fit (beyond about 4096 x 4096) are rejected with
+ * BGT_ERR_LIMIT.  No cudaMalloc or cudaFree is called.  Calls share the
+ * array: they are serialised by a process-wide lock and each returns after
+ * its work on `stream` finished; work arranged to overlap on the GPU would
+ * race on the array.  The first call on a device looks up the array's
+ * address; make it before any stream capture. */
+int bgt_thin2d_device_noalloc(int device, int dtype, const void *d_in, int width, int height, void *d_out,
+                              void *stream);
+
 /* ---- centreline extraction (host buffers, synchronous) ----------------
  * Replace CenterlineExtraction<T> (2D/CenterlineExtraction.h:25-28,
  * 3D/CenterlineExctraction.h:26-29): thinning, segment extraction, pruning
