@@ -84,6 +84,14 @@ int oracle_binarise(int dtype, const void *src, int64_t n, int dims, uint8_t *ds
 uint64_t oracle_rule2d(int dir, const uint64_t *x);
 uint64_t oracle_rule3d(int dir, const uint64_t *nb);
 
+/* Exhaustive comparison of the 3D rule of direction dir (0..5 = U,N,E,D,S,W)
+ * with a rule function of the reference's signature
+ * (val, n[26] in the reference's neighbour order, prev) over all 2^26
+ * neighbourhoods of a foreground centre.  Returns the number of
+ * neighbourhoods on which the deletable sets differ. */
+typedef unsigned int (*ref_rule3d_fn)(int dir, unsigned int val, unsigned int *n26, unsigned int prev);
+long long oracle_rule3d_exhaustive(int dir, ref_rule3d_fn ref);
+
 #ifdef __cplusplus
 }
 #endif

@@ -235,6 +235,16 @@ def rule3d(direction: int, nb27: np.ndarray) -> np.ndarray:
     return np.uint64(lib().oracle_rule3d(direction, a.ctypes.data_as(C.POINTER(C.c_uint64))))
 
 
+def rule3d_exhaustive_vs_ref(direction: int) -> int:
+    """Bits on which the restated 3D rule and the reference's own rule
+    function differ, over all 2^26 neighbourhoods (needs oracle/_ref)."""
+    L = lib()
+    L.oracle_rule3d_exhaustive.argtypes = [C.c_int, C.c_void_p]
+    L.oracle_rule3d_exhaustive.restype = C.c_longlong
+    fn = C.cast(ref("3d").ref3d_rule, C.c_void_p)
+    return int(L.oracle_rule3d_exhaustive(direction, fn))
+
+
 # --------------------------------------------------------------------------
 # The reference's own code (built only where the reference tree exists).
 # --------------------------------------------------------------------------

@@ -211,6 +211,35 @@ uint64_t oracle_rule3d(int dir, const uint64_t *nb)
     return up_template(loc);
 }
 
+/* 32 neighbourhoods per call: neighbour i < 5 varies across the 32 bit
+ * lanes, neighbours 5..25 (reference order, centre skipped) follow the bits
+ * of `hi`. */
+long long oracle_rule3d_exhaustive(int dir, ref_rule3d_fn ref)
+{
+    build_frames();
+    long long bad = 0;
+    unsigned int lane_pat[5];
+    for (int i = 0; i < 5; i++) {
+        unsigned int w = 0;
+        for (int l = 0; l < 32; l++)
+            if ((l >> i) & 1) w |= 1u << l;
+        lane_pat[i] = w;
+    }
+    for (uint32_t hi = 0; hi < (1u << 21); hi++) {
+        unsigned int n[26];
+        w64 g[27], loc[27];
+        for (int i = 0; i < 26; i++)
+            n[i] = i < 5 ? lane_pat[i] : (((hi >> (i - 5)) & 1) ? 0xffffffffu : 0u);
+        for (int p = 0, i = 0; p < 27; p++) g[p] = p == 13 ? 0xffffffffu : (w64)n[i++];
+        for (int i = 0; i < 27; i++) loc[i] = g[frame_map[dir][i]];
+        const unsigned int mine = (unsigned int)up_template(loc);
+        /* reference returns val with the deletable bits cleared (prev = 0) */
+        const unsigned int theirs = ~ref(dir, 0xffffffffu, n, 0u);
+        bad += __builtin_popcount(mine ^ theirs);
+    }
+    return bad;
+}
+
 int oracle_thin3d(uint8_t *vol, int w, int h, int d, int nthreads)
 {
     if (w <= 0 || h <= 0 || d <= 0) return 0;
