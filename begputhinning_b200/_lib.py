@@ -17,8 +17,11 @@ EXPORTS = [
     "bgt_centerline2d", "bgt_centerline3d", "bgt_free",
     "bgt_segments2d_device", "bgt_segments3d_device",
     "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
+    "bgt_batch_reserve", "bgt_batch_reset", "bgt_batch_set_grid",
     "bgt_batch_set_io", "bgt_batch_run", "bgt_batch_instance_stats", "bgt_batch_device_bytes", "bgt_batch_work", "bgt_batch_stage_ms",
     "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe",
+    "bgt_server_create", "bgt_server_submit", "bgt_server_poll", "bgt_server_drain", "bgt_server_stats",
+    "bgt_server_reset_stats", "bgt_server_destroy",
 ]
 
 
@@ -65,6 +68,9 @@ def _declare(L):
         "bgt_batch_add2d": [vp, I, I, I, ip],
         "bgt_batch_add3d": [vp, I, I, I, I, ip],
         "bgt_batch_finalize": [vp],
+        "bgt_batch_reserve": [vp, C.c_size_t],
+        "bgt_batch_reset": [vp],
+        "bgt_batch_set_grid": [vp, I],
         "bgt_batch_set_io": [vp, I, I, vp, vp],
         "bgt_batch_run": [vp, I, I],
         "bgt_batch_instance_stats": [vp, I, ip, ip, ip],
@@ -76,6 +82,14 @@ def _declare(L):
         "bgt_tune_get": [I, I, ip],
         "bgt_cfg_list": [I, ip, I, ip],
         "bgt_cfg_describe": [I, ip, ip, ip, ip, ip, ip],
+        "bgt_server_create": [I, C.c_size_t, C.POINTER(vp)],
+        "bgt_server_submit": [vp, I, vp, I, I, I, vp, C.POINTER(C.c_ulonglong)],
+        "bgt_server_poll": [vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double), ip, I, ip],
+        "bgt_server_drain": [vp, C.c_double],
+        "bgt_server_stats": [vp, I, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                             C.POINTER(C.c_ulonglong)],
+        "bgt_server_reset_stats": [vp],
+        "bgt_server_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

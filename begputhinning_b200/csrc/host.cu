@@ -287,9 +287,17 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     const size_t off_inst = off; off = align_up(off + (size_t)N * sizeof(Inst), 256);
     const size_t off_tmap = off; off = align_up(off + (size_t)N * 2 * sizeof(CUtensorMap), 256);
     const size_t off_flag = off; off = align_up(off + 64, 256);
-    cudaError_t e = cudaMalloc(&b->pool, off);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch pool)");
-    b->pool_bytes = off;
+    cudaError_t e;
+    if (b->reserved) {
+        // a reserved pool is re-laid-out for every set of instances, never reallocated
+        if (off > b->pool_bytes)
+            return fail(BGT_ERR_LIMIT, "batch needs %zu bytes, the reserved pool holds %zu", off, b->pool_bytes);
+    } else {
+        e = cudaMalloc(&b->pool, off);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(batch pool)");
+        b->pool_bytes = off;
+    }
+    b->used_bytes = off;
     char *P = (char *)b->pool;
     b->d_sched = (Sched *)(P + off_sched);
     b->d_seq = (unsigned *)(P + off_seq);
@@ -300,7 +308,8 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     b->d_lc = P + off_lc;
     b->d_io = (IODesc *)(P + off_io);
     b->cap = cap;
-    std::vector<CUtensorMap> maps((size_t)N * 2);
+    std::vector<CUtensorMap> &maps = b->maps;
+    maps.assign((size_t)N * 2, CUtensorMap());
     for (int i = 0; i < N; i++) {
         Inst &in = b->h[i];
         const Offs &o = offs[i];
@@ -315,35 +324,89 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
         int rc = encode_map(&maps[2 * i], in, c, in.buf[0]);
         if (rc == BGT_OK) rc = encode_map(&maps[2 * i + 1], in, c, in.buf[1]);
         if (rc != BGT_OK) {
-            batch_free_device(b);
+            if (!b->reserved) batch_free_device(b);
             return rc;
         }
     }
-    e = cudaMemcpy(b->d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+    // tables are uploaded in stream order from host copies the batch keeps
+    cudaStream_t st = b->ctx->stream;
+    e = cudaMemcpyAsync(b->d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = cudaMemcpy(b->d_insts, b->h.data(), (size_t)N * sizeof(Inst), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(b->d_insts, b->h.data(), (size_t)N * sizeof(Inst), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
-        batch_free_device(b);
-        return cuda_fail(e, "cudaMemcpy(batch tables)");
+        if (!b->reserved) batch_free_device(b);
+        return cuda_fail(e, "batch table upload");
     }
     b->smem = max_smem;
-    e = engine_set_smem(std::max(max_smem, 48 * 1024));
+    // one value for every batch (the largest configuration), so concurrent
+    // batches never race on the kernel attribute
+    e = engine_set_smem(max_cfg_smem());
     if (e != cudaSuccess) {
-        batch_free_device(b);
+        if (!b->reserved) batch_free_device(b);
         return cuda_fail(e, "cudaFuncSetAttribute");
     }
     const int per_sm = std::max(1, engine_max_blocks_per_sm(max_smem));
     b->grid = b->ctx->sms * per_sm;
+    if (b->grid_cap > 0) b->grid = std::min(b->grid, b->grid_cap);
     for (auto &ev : b->ev) {
+        if (ev) continue;
         e = cudaEventCreate(&ev);
         if (e != cudaSuccess) {
-            batch_free_device(b);
+            if (!b->reserved) batch_free_device(b);
             return cuda_fail(e, "cudaEventCreate");
         }
     }
     b->io.assign(N, IO());
     b->stats.assign(N, Stat());
     b->finalized = true;
+    return BGT_OK;
+}
+
+// Pre-allocate `bytes` of device pool: later finalize calls lay the batch out
+// in it (reset + add + finalize reuses it without any allocation) and fail
+// with BGT_ERR_LIMIT when a set of instances does not fit.
+extern "C" int bgt_batch_reserve(bgt_batch *b, size_t bytes)
+{
+    if (!b) return fail(BGT_ERR_ARG, "null batch");
+    if (b->finalized || b->pool) return fail(BGT_ERR_STATE, "reserve before the first finalize");
+    cudaSetDevice(b->ctx->device);
+    cudaError_t e = cudaMalloc(&b->pool, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(reserved batch pool)");
+    b->pool_bytes = bytes;
+    b->reserved = true;
+    return BGT_OK;
+}
+
+// Drop the instances (after the last run finished on the batch's stream);
+// a reserved pool and the events are kept.
+extern "C" int bgt_batch_reset(bgt_batch *b)
+{
+    if (!b) return fail(BGT_ERR_ARG, "null batch");
+    if (!b->reserved && b->pool) {
+        cudaStreamSynchronize(b->ctx->stream);
+        cudaFree(b->pool);
+        b->pool = nullptr;
+        b->pool_bytes = 0;
+    }
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+    b->graph_valid = false;
+    b->items.clear();
+    b->h.clear();
+    b->io.clear();
+    b->stats.clear();
+    b->io_dirty = true;
+    b->finalized = false;
+    b->stats_valid = false;
+    return BGT_OK;
+}
+
+// Upper bound on the engine's CTAs (0: one full wave of the device), so that
+// batches on several streams share the SMs.  Applies from the next finalize.
+extern "C" int bgt_batch_set_grid(bgt_batch *b, int ctas)
+{
+    if (!b || ctas < 0) return fail(BGT_ERR_ARG, "bad argument");
+    b->grid_cap = ctas;
     return BGT_OK;
 }
 
@@ -422,13 +485,14 @@ __global__ void sched_reset_kernel(Sched *S, unsigned *seq, int4 *item, unsigned
     }
 }
 
-// Upload the per-instance I/O table used by the batch-wide pack/unpack
-// (synchronous; done before any capture).
+// Upload the per-instance I/O table used by the batch-wide pack/unpack, in
+// stream order from a host copy the batch keeps (done before any capture).
 static int upload_io(bgt_batch *b)
 {
     if (!b->io_dirty) return BGT_OK;
     const int N = (int)b->items.size();
-    std::vector<IODesc> io(N);
+    std::vector<IODesc> &io = b->io_host;
+    io.assign(N, IODesc());
     long long w = 0, g = 0;
     for (int i = 0; i < N; i++) {
         const Inst &in = b->h[i];
@@ -451,7 +515,8 @@ static int upload_io(bgt_batch *b)
     b->unpack_words = g;
     b->any_out = false;
     for (int i = 0; i < N; i++) b->any_out |= b->io[i].out != nullptr;
-    cudaError_t e = cudaMemcpy(b->d_io, io.data(), (size_t)N * sizeof(IODesc), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(b->d_io, io.data(), (size_t)N * sizeof(IODesc), cudaMemcpyHostToDevice,
+                                    b->ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "I/O table upload");
     b->io_dirty = false;
     return BGT_OK;

@@ -10,6 +10,7 @@
 
 #include "bgt_capi.h"
 #include "common.cuh"
+#include "kernels.cuh"
 
 struct bgt_batch;
 
@@ -79,6 +80,11 @@ struct bgt_batch {
     int last_mode = 0;
     void *pool = nullptr;
     size_t pool_bytes = 0;
+    size_t used_bytes = 0;
+    bool reserved = false;              // pool pre-allocated by bgt_batch_reserve
+    int grid_cap = 0;                   // engine CTA cap (0: full device)
+    std::vector<CUtensorMap> maps;      // host copies of uploaded tables (kept
+    std::vector<bgt::IODesc> io_host;   // alive for stream-ordered uploads)
     bgt::Sched *d_sched = nullptr;
     unsigned *d_seq = nullptr;
     int4 *d_item = nullptr;

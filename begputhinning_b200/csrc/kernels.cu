@@ -47,6 +47,13 @@ const CfgInfo *cfg_info(int id)
         if (c.id == id) return &c;
     return nullptr;
 }
+int max_cfg_smem()
+{
+    int m = 0;
+    for (const auto &c : kCfgs) m = std::max(m, c.smem);
+    return m;
+}
+
 const int *cfg_ids_2d(int *n) { *n = 8; return kIds2d; }
 const int *cfg_ids_3d(int *n) { *n = 3; return kIds3d; }
 

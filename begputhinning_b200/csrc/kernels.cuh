@@ -19,6 +19,7 @@ struct CfgInfo {
     int box[3];       // TMA box (words, rows, planes)
 };
 const CfgInfo *cfg_info(int id);  // nullptr if unknown
+int max_cfg_smem();               // largest dynamic shared memory of any configuration
 const int *cfg_ids_2d(int *n);
 const int *cfg_ids_3d(int *n);
 

@@ -130,6 +130,15 @@ int bgt_batch_destroy(bgt_batch *b);
 int bgt_batch_add2d(bgt_batch *b, int width, int height, int cfg, int *id);
 int bgt_batch_add3d(bgt_batch *b, int width, int height, int depth, int cfg, int *id);
 int bgt_batch_finalize(bgt_batch *b);
+/* Reuse without allocation: reserve a device pool once (before the first
+ * finalize); reset drops the instances (keeping the pool) so the batch can
+ * be refilled and finalized again; a set of instances that does not fit
+ * the reserved pool fails finalize with BGT_ERR_LIMIT. */
+int bgt_batch_reserve(bgt_batch *b, size_t bytes);
+int bgt_batch_reset(bgt_batch *b);
+/* Cap the persistent engine's CTAs (0 = a full wave of the device) so
+ * batches running on several streams share the SMs. */
+int bgt_batch_set_grid(bgt_batch *b, int ctas);
 int bgt_batch_set_io(bgt_batch *b, int id, int dtype, const void *d_in, void *d_out);
 /* mode 0: persistent engine (optionally replayed as a CUDA graph when
  * use_graph != 0); mode 1: plain path, one launch per pass per instance with
@@ -146,6 +155,29 @@ int bgt_batch_work(bgt_batch *b, unsigned long long *tiles, unsigned long long *
 /* device milliseconds of the last engine run's stages (CUDA events on the
  * batch's stream): pack, engine (the persistent thinning kernel), unpack */
 int bgt_batch_stage_ms(bgt_batch *b, float *pack_ms, float *engine_ms, float *unpack_ms);
+
+/* ---- serving -------------------------------------------------------------
+ * A request loop over the batch engine.  Requests (2D frames: depth 1; 3D
+ * volumes: depth > 1) are submitted from any host thread with host buffers
+ * (pinned memory keeps the copies asynchronous) that must stay valid until
+ * the request completes.  A dispatcher thread admits waiting requests into
+ * free device slots of their lane (frames: high-priority streams; volumes:
+ * low-priority streams) when the slot has room, and launches them while
+ * earlier launches still run (continuous batching); device memory is
+ * reserved once at creation within hbm_budget_bytes and stays resident.
+ * Latency = submit to output in host memory. */
+typedef struct bgt_server bgt_server;
+int bgt_server_create(int device, size_t hbm_budget_bytes, bgt_server **out);
+int bgt_server_submit(bgt_server *s, int dtype, const void *host_in, int width, int height, int depth,
+                      void *host_out, unsigned long long *ticket);
+/* completed requests since the last poll (ticket, latency in ms, status) */
+int bgt_server_poll(bgt_server *s, unsigned long long *tickets, double *latency_ms, int *status, int cap, int *n);
+int bgt_server_drain(bgt_server *s, double timeout_s);
+/* lane 0 = frames, 1 = volumes: latency percentiles, Mvoxel/s, completed count */
+int bgt_server_stats(bgt_server *s, int lane, double *p50_ms, double *p99_ms, double *mvox_per_s,
+                     unsigned long long *completed);
+int bgt_server_reset_stats(bgt_server *s);
+int bgt_server_destroy(bgt_server *s);
 
 /* ---- tile configurations and the autotuner's table --------------------
  * The autotuner (begputhinning_b200/tune.py) times the configurations on
