@@ -55,7 +55,10 @@ def parse():
     p.add_argument("--n2d", type=int, default=512, help="2D instances per GPU (smaller only for profiling)")
     p.add_argument("--n3d", type=int, default=32, help="3D instances per GPU (smaller only for profiling)")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--tune", default="cache", choices=["cache", "run", "off"],
+                   help="tile configurations: cached autotuner table (tune when absent), retune, or defaults")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-seconds", type=float, default=4.0, help="measured seconds of the serving run")
     return p.parse_args()
 
 
@@ -183,6 +186,14 @@ def run_bgt(args, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     items = workload(args.seed + 1000 * rank, args.n2d, args.n3d)
+    from begputhinning_b200 import tune
+    table = {}
+    if args.tune == "cache":
+        table = tune.load_cache(local)
+    if args.tune == "run" or (args.tune == "cache" and not table):
+        table = tune.autotune(items, device=local)["table"]
+        if rank == 0:
+            tune.save_cache(table, local)
     sizes = [it.size for it in items]
     units = int(sum(sizes))
     total = sum(sizes)
@@ -329,6 +340,7 @@ def run_bgt(args, rank, world, local):
                    "voxels_per_gpu": units, "input_bytes_per_gpu": total,
                    "l2": "inputs larger than L2 (uint8 inputs and outputs of several hundred MB per step)",
                    "step": "batch-wide pack + persistent engine + batch-wide unpack, one CUDA graph",
+                   "tile_configs": {f"{d}D class {c}": v for (d, c), v in sorted(table.items())},
                    "parallelism": f"instances per rank, {world} rank(s), no collective"},
         "e2e": {"value": units_all / (e2e_max * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": total,
                 "d2h_bytes_per_step": total,
@@ -345,10 +357,24 @@ def run_bgt(args, rank, world, local):
     if plain:
         line["plain"] = plain
         line["batched_over_plain"] = line["value"] / plain["value"]
-    if world == 1:
-        line["cpu_baseline"] = cpu_baseline(items, args.cpu_seconds)
     b.close()
     ctx.close()
+    if world == 1:
+        line["cpu_baseline"] = cpu_baseline(items, args.cpu_seconds)
+        if not args.no_serve:
+            from begputhinning_b200.serve import run_workload
+            s = run_workload(duration_s=args.serve_seconds, device=local)
+            line["serving"] = {
+                "workload": "Poisson arrivals: 16 streams x 30 fps of 1024x1024 frames (70% of requests) + "
+                            "tree volumes with sides U[128,320] (30%); 64 GB HBM budget",
+                "frame_p50_ms": s["frames"]["p50_ms"], "frame_p99_ms": s["frames"]["p99_ms"],
+                "volume_p50_ms": s["volumes"]["p50_ms"], "volume_p99_ms": s["volumes"]["p99_ms"],
+                "frames_completed": s["frames"]["completed"], "volumes_completed": s["volumes"]["completed"],
+                "frame_mvoxel_per_s": s["frames"]["mvoxel_per_s"],
+                "volume_mvoxel_per_s": s["volumes"]["mvoxel_per_s"],
+                "offered_requests_per_s": s["offered_rate_per_s"], "measured_seconds": s["duration_s"],
+                "latency": "submission to output in pinned host memory",
+            }
     return line
 
 
