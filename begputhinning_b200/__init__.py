@@ -4,8 +4,8 @@ for the Thinning2D / Thinning3D / CenterlineExtraction entry points of
 BEGPUThinning.  The compute path is libbgt.so (hand-written sm_100a CUDA
 behind a C ABI, include/bgt_capi.h); this package is the Python host side."""
 from ._lib import BGTError, lib
-from .api import (Batch, CenterlineExtraction, Context, ExtractSegmentsV, Segments, Thinning2D, Thinning3D,
-                  cfg_describe, cfg_list, default_context, thin_device)
+from .api import (Batch, CenterlineExtraction, Context, ExtractSegmentsV, PipelinedBatch, Segments, Thinning2D,
+                  Thinning3D, cfg_describe, cfg_list, default_context, thin_device)
 
-__all__ = ["BGTError", "lib", "Batch", "CenterlineExtraction", "Context", "ExtractSegmentsV", "Segments",
+__all__ = ["BGTError", "lib", "Batch", "CenterlineExtraction", "Context", "ExtractSegmentsV", "PipelinedBatch", "Segments",
            "Thinning2D", "Thinning3D", "cfg_describe", "cfg_list", "default_context", "thin_device"]

@@ -303,6 +303,83 @@ class Batch:
             pass
 
 
+class PipelinedBatch:
+    """Host-to-host thinning of many instances with transfers overlapped.
+
+    The instances (in the given order, as contiguous byte ranges of one
+    uint8 host input and one host output, both pinned) are split into
+    `chunks` consecutive groups of similar size.  Each group is a Batch of
+    its own; group c is copied in on a copy stream, thinned on the compute
+    stream once its copy finished, and copied out on a third stream, so the
+    copy-in of later groups and the copy-out of earlier ones run during the
+    thinning of the current group.  Put instances with long chains of passes
+    (3D volumes) first: their group starts first."""
+
+    def __init__(self, shapes, chunks: int = 4, device: int = 0):
+        import numpy as np
+        import torch
+        self.device = device
+        self.dev = torch.device("cuda", device)
+        self.shapes = [tuple(s) for s in shapes]
+        sizes = [int(np.prod(s)) for s in self.shapes]
+        self.offs = np.cumsum([0] + sizes)
+        self.total = int(self.offs[-1])
+        target = self.total / max(1, chunks)
+        bounds, acc, start = [], 0, 0
+        for i, s in enumerate(sizes):
+            acc += s
+            if acc >= target * (len(bounds) + 1) and len(bounds) < chunks - 1:
+                bounds.append((start, i + 1))
+                start = i + 1
+        if start < len(sizes):
+            bounds.append((start, len(sizes)))
+        self.groups = bounds
+        self.dev_in = torch.empty(self.total, dtype=torch.uint8, device=self.dev)
+        self.dev_out = torch.empty(self.total, dtype=torch.uint8, device=self.dev)
+        self.s_in = torch.cuda.Stream(self.dev)
+        self.s_comp = torch.cuda.Stream(self.dev)
+        self.s_out = torch.cuda.Stream(self.dev)
+        self.ctx = Context(device)
+        self.ctx.set_stream(self.s_comp)
+        self.batches = []
+        for a, b in self.groups:
+            bt = Batch(self.ctx)
+            ids = [bt.add(self.shapes[i]) for i in range(a, b)]
+            bt.finalize()
+            for j, i in zip(ids, range(a, b)):
+                lo, hi = int(self.offs[i]), int(self.offs[i + 1])
+                bt.set_io(j, self.dev_in[lo:hi], self.dev_out[lo:hi])
+            self.batches.append(bt)
+        torch.cuda.synchronize(self.dev)
+
+    def run(self, host_in, host_out) -> None:
+        """Enqueue one host-to-host pass (no synchronisation)."""
+        import torch
+        for (a, b), bt in zip(self.groups, self.batches):
+            lo, hi = int(self.offs[a]), int(self.offs[b])
+            e_in = torch.cuda.Event()
+            with torch.cuda.stream(self.s_in):
+                self.dev_in[lo:hi].copy_(host_in[lo:hi], non_blocking=True)
+                e_in.record(self.s_in)
+            self.s_comp.wait_event(e_in)
+            bt.run(graph=True, sync=False)
+            e_c = torch.cuda.Event()
+            e_c.record(self.s_comp)
+            self.s_out.wait_event(e_c)
+            with torch.cuda.stream(self.s_out):
+                host_out[lo:hi].copy_(self.dev_out[lo:hi], non_blocking=True)
+        # the next pass may overwrite device inputs only after this pass read them
+        e_end = torch.cuda.Event()
+        e_end.record(self.s_out)
+        self.s_in.wait_event(e_end)
+
+    def close(self):
+        for bt in self.batches:
+            bt.close()
+        self.batches = []
+        self.ctx.close()
+
+
 def cfg_list(dims: int):
     ids = (C.c_int * 32)()
     n = C.c_int()

@@ -196,6 +196,8 @@ static int batch_add(bgt_batch *b, int dims, int W, int H, int D, int cfg, int *
     if (b->finalized) return fail(BGT_ERR_STATE, "batch already finalized");
     if (W < 1 || H < 1 || D < 1 || W > 32767 || H > 32767 || D > 32767)
         return fail(BGT_ERR_ARG, "size %dx%dx%d out of range (1..32767 per axis)", W, H, D);
+    if ((long long)W * H * D >= (1LL << 31))
+        return fail(BGT_ERR_LIMIT, "instance of %lld pixels: the limit is 2^31 - 1", (long long)W * H * D);
     if (cfg >= 0) {
         const CfgInfo *c = cfg_info(cfg);
         if (!c || c->dims != dims) return fail(BGT_ERR_ARG, "configuration %d is not a %dD configuration", cfg, dims);
@@ -509,7 +511,15 @@ static int upload_io(bgt_batch *b)
         io[i].wbegin = w;
         io[i].gbegin = g;
         w += (long long)in.P * in.H * in.D;
-        g += (long long)((in.W + 31) / 32) * in.H * in.D;
+        if (dtype_size(s.dtype) == 1 && s.out) {
+            // unpack unit: 16-byte-aligned chunk of the output
+            const uintptr_t o = reinterpret_cast<uintptr_t>(s.out);
+            const uintptr_t end = o + (uintptr_t)in.W * in.H * in.D;
+            g += (long long)((end - (o & ~uintptr_t(15)) + 15) / 16);
+        } else {
+            // unpack unit: packed word (rows x ceil(W/32))
+            g += (long long)((in.W + 31) / 32) * in.H * in.D;
+        }
     }
     b->pack_words = w;
     b->unpack_words = g;

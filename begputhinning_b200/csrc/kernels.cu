@@ -18,6 +18,11 @@ using C2_1_28 = Cfg2D<1, 28, 4>;
 using C2_2_28 = Cfg2D<2, 28, 4>;
 using C2_4_28 = Cfg2D<4, 28, 4>;
 using C2_8_28 = Cfg2D<8, 28, 4>;
+using X2_4_12 = Cfg2DX<4, 12, 4>;
+using X2_8_12 = Cfg2DX<8, 12, 4>;
+using X2_16_12 = Cfg2DX<16, 12, 4>;
+using X2_4_28 = Cfg2DX<4, 28, 4>;
+using X2_8_28 = Cfg2DX<8, 28, 4>;
 using C3_8 = Cfg3D<4, 8>;
 using C3_16 = Cfg3D<4, 16>;
 using C3_32 = Cfg3D<4, 32>;
@@ -36,9 +41,10 @@ constexpr CfgInfo info3d(int id)
 static const CfgInfo kCfgs[] = {
     info2d<C2_1_12>(0), info2d<C2_2_12>(1), info2d<C2_4_12>(2), info2d<C2_8_12>(3),
     info2d<C2_1_28>(4), info2d<C2_2_28>(5), info2d<C2_4_28>(6), info2d<C2_8_28>(7),
+    info2d<X2_4_12>(8), info2d<X2_8_12>(9), info2d<X2_16_12>(10), info2d<X2_4_28>(11), info2d<X2_8_28>(12),
     info3d<C3_8>(16),   info3d<C3_16>(17),  info3d<C3_32>(18),
 };
-static const int kIds2d[] = {0, 1, 2, 3, 4, 5, 6, 7};
+static const int kIds2d[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12};
 static const int kIds3d[] = {16, 17, 18};
 
 const CfgInfo *cfg_info(int id)
@@ -54,8 +60,8 @@ int max_cfg_smem()
     return m;
 }
 
-const int *cfg_ids_2d(int *n) { *n = 8; return kIds2d; }
-const int *cfg_ids_3d(int *n) { *n = 3; return kIds3d; }
+const int *cfg_ids_2d(int *n) { *n = (int)(sizeof(kIds2d) / sizeof(kIds2d[0])); return kIds2d; }
+const int *cfg_ids_3d(int *n) { *n = (int)(sizeof(kIds3d) / sizeof(kIds3d[0])); return kIds3d; }
 
 constexpr int kThreads = 128;
 
@@ -78,6 +84,8 @@ __device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem, uint64
         return tile2d<C, 0>(in, q, tile, smem, bar, parity, err);
 #define CASE2_K4(ID, C) \
     case ID: return tile2d<C, 0>(in, q, tile, smem, bar, parity, err);
+#define CASE2X(ID, C) \
+    case ID: return tile2dx<C, 0>(in, q, tile, smem, bar, parity, err);
 #define CASE3(ID, C)                                                             \
     case ID:                                                                     \
         switch (q % 6) {                                                         \
@@ -96,12 +104,18 @@ __device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem, uint64
         CASE2_K2(5, C2_2_28)
         CASE2_K4(6, C2_4_28)
         CASE2_K4(7, C2_8_28)
+        CASE2X(8, X2_4_12)
+        CASE2X(9, X2_8_12)
+        CASE2X(10, X2_16_12)
+        CASE2X(11, X2_4_28)
+        CASE2X(12, X2_8_28)
         CASE3(16, C3_8)
         CASE3(17, C3_16)
         CASE3(18, C3_32)
 #undef CASE2_K1
 #undef CASE2_K2
 #undef CASE2_K4
+#undef CASE2X
 #undef CASE3
     default:
         return false;
@@ -296,6 +310,12 @@ __device__ __forceinline__ uint32_t pack_word_mode(const T *p, int n, int mode, 
                                                                : pack_word<T, 2>(p, n, room);
 }
 
+__device__ __forceinline__ int dtype_bytes(int dtype)
+{
+    return dtype == BGT_F64 ? 8 : (dtype == BGT_U32 || dtype == BGT_I32 || dtype == BGT_F32) ? 4
+                                  : (dtype == BGT_U16 || dtype == BGT_I16) ? 2 : 1;
+}
+
 __device__ __forceinline__ int find_io(const IODesc *io, int n, long long g, bool unpack)
 {
     int lo = 0, hi = n - 1;
@@ -310,14 +330,25 @@ __device__ __forceinline__ int find_io(const IODesc *io, int n, long long g, boo
 __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__restrict__ io, int n,
                                 long long total)
 {
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
-         g += (long long)gridDim.x * blockDim.x) {
-        const IODesc &d = io[find_io(io, n, g, false)];
+    int k = -1;
+    long long kb = 0, ke = 0;
+    // each block takes one contiguous range, so consecutive units of a thread
+    // stay in the same instance and the instance lookup is rarely repeated
+    const long long per = (total + gridDim.x - 1) / gridDim.x;
+    const long long g_end = min(total, per * (blockIdx.x + 1));
+    for (long long g = per * blockIdx.x + threadIdx.x; g < g_end; g += blockDim.x) {
+        if (g < kb || g >= ke) {  // instance lookup only when leaving the cached range
+            k = find_io(io, n, g, false);
+            kb = io[k].wbegin;
+            ke = k + 1 < n ? io[k + 1].wbegin : total;
+        }
+        const IODesc &d = io[k];
         const Inst &in = insts[d.inst];
-        const long long i = g - d.wbegin;
-        const long long row = i / in.P;
-        const int j = (int)(i - row * in.P);
-        const int y = (int)(row % in.H), z = (int)(row / in.H);
+        // 32-bit index math: an instance has fewer than 2^31 packed words
+        const unsigned i = (unsigned)(g - d.wbegin);
+        const unsigned row = i / (unsigned)in.P;
+        const int j = (int)(i - row * (unsigned)in.P);
+        const int z = (int)(row / (unsigned)in.H), y = (int)(row - (unsigned)z * (unsigned)in.H);
         const int x0 = j * 32;
         uint32_t w = 0;
         if (x0 < d.inW && y < d.inH && z < d.inD) {
@@ -383,14 +414,76 @@ __device__ __forceinline__ void unpack_word(uint32_t w, T *o, int n)
     for (int b = 0; b < n; b++) o[b] = (T)((w >> b) & 1u);
 }
 
+// One-byte outputs: unit = one 16-byte-aligned chunk of the output (absolute
+// address), written with one 128-bit store when the chunk lies inside the
+// instance's output, bytewise at its two ends.  Each byte is pixel
+// (row, x) of the flat index; rows may change inside a chunk.
+__device__ __forceinline__ void unpack_chunk16(const Inst &in, const IODesc &d, long long c)
+{
+    const uintptr_t out = reinterpret_cast<uintptr_t>(d.out);
+    const long long n = (long long)in.W * in.H * in.D;
+    const uintptr_t a = (out & ~uintptr_t(15)) + (uintptr_t)c * 16u;
+    const long long lo = (long long)(a > out ? a - out : 0);  // first flat index in the chunk
+    const long long hi = min((long long)(a + 16 - out), n);   // one past the last
+    // flat indices of one instance stay below 2^31 (sizes are capped at 32767
+    // per axis and the batch limits an instance to < 2^31 pixels)
+    unsigned row = (unsigned)lo / (unsigned)in.W;
+    int x = (int)((unsigned)lo - row * (unsigned)in.W);
+    if (hi - lo == 16 && a >= out && x + 16 <= in.W) {
+        // whole chunk inside one row: 16 consecutive bits, expanded 4 at a time
+        const uint32_t *r = in.buf[0] + (size_t)row * in.P;
+        const uint32_t w0 = __ldcg(r + (x >> 5));
+        const uint32_t w1 = ((x & 31) > 16) ? __ldcg(r + (x >> 5) + 1) : 0u;
+        const uint32_t bits = __funnelshift_r(w0, w1, x & 31);
+        *reinterpret_cast<uint4 *>(a) = make_uint4(bits4_to_bytes(bits & 15u), bits4_to_bytes((bits >> 4) & 15u),
+                                                   bits4_to_bytes((bits >> 8) & 15u),
+                                                   bits4_to_bytes((bits >> 12) & 15u));
+        return;
+    }
+    uint32_t word = __ldcg(in.buf[0] + (size_t)row * in.P + (x >> 5));
+    uint32_t bytes[4] = {0u, 0u, 0u, 0u};
+    const int first = (int)((out + lo) - a);  // byte position of flat index lo in the chunk
+    for (long long f = lo; f < hi; f++) {
+        const int pos = first + (int)(f - lo);
+        bytes[pos >> 2] |= ((word >> (x & 31)) & 1u) << (8 * (pos & 3));
+        if (++x == in.W) {
+            x = 0;
+            row++;
+            if (f + 1 < hi) word = __ldcg(in.buf[0] + (size_t)row * in.P);
+        } else if ((x & 31) == 0 && f + 1 < hi) {
+            word = __ldcg(in.buf[0] + (size_t)row * in.P + (x >> 5));
+        }
+    }
+    if (first == 0 && hi - lo == 16) {
+        *reinterpret_cast<uint4 *>(a) = make_uint4(bytes[0], bytes[1], bytes[2], bytes[3]);
+    } else {
+        uint8_t *ob = reinterpret_cast<uint8_t *>(a);
+        for (int pos = first; pos < first + (int)(hi - lo); pos++) ob[pos] = (uint8_t)(bytes[pos >> 2] >> (8 * (pos & 3)));
+    }
+}
+
 __global__ void unpack_all_kernel(const Inst *__restrict__ insts, const IODesc *__restrict__ io, int n,
                                   long long total)
 {
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
-         g += (long long)gridDim.x * blockDim.x) {
-        const IODesc &d = io[find_io(io, n, g, true)];
+    int k = -1;
+    long long kb = 0, ke = 0;
+    // each block takes one contiguous range, so consecutive units of a thread
+    // stay in the same instance and the instance lookup is rarely repeated
+    const long long per = (total + gridDim.x - 1) / gridDim.x;
+    const long long g_end = min(total, per * (blockIdx.x + 1));
+    for (long long g = per * blockIdx.x + threadIdx.x; g < g_end; g += blockDim.x) {
+        if (g < kb || g >= ke) {  // instance lookup only when leaving the cached range
+            k = find_io(io, n, g, true);
+            kb = io[k].gbegin;
+            ke = k + 1 < n ? io[k + 1].gbegin : total;
+        }
+        const IODesc &d = io[k];
         if (!d.out) continue;
         const Inst &in = insts[d.inst];
+        if (dtype_bytes(d.dtype) == 1) {
+            unpack_chunk16(in, d, g - d.gbegin);
+            continue;
+        }
         const int wwords = (in.W + 31) >> 5;
         const long long i = g - d.gbegin;
         const long long row = i / wwords;

@@ -139,6 +139,144 @@ __device__ bool tile2d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t
     return any;
 }
 
+// ------------------------------------------- 2D, shared warp edges -------
+// Variant: the NW warps of a tile form one band of 32*NW rows.  After every
+// subiteration each warp publishes its first and last row (lanes 0 and 31)
+// in shared memory; the warp below/above reads them in place of the shuffle
+// that would otherwise wrap inside the warp.  Only the band's outer K rows
+// are halo: 32*NW - 2K core rows instead of NW*(32 - 2K).
+template <int K, int S, int NW>
+struct Cfg2DX {
+    static constexpr int kK = K, kS = S, kNW = NW;
+    static constexpr int TH = 32 * NW - 2 * K;  // core rows per tile
+    static constexpr int BW = S + 8;            // box width in words
+    static constexpr int BH = 32 * NW;          // box rows
+    static constexpr int EX = S + 2;            // words of an exchanged row
+    static constexpr int SMEM = BW * BH * 4 + 2 * 2 * NW * EX * 4;
+    static constexpr int THREADS = NW * 32;
+    static_assert(S % 4 == 0, "S must be a multiple of 4");
+    static_assert(BW <= 256 && BH <= 256, "TMA box too large");
+};
+
+// One subiteration with edge rows from shared memory: ex_up is the row above
+// lane 0 (warps > 0), ex_dn the row below lane 31 (warps < NW-1).
+template <int S, int DIR>
+__device__ __forceinline__ void subit2d_x(uint32_t (&v)[S + 2], uint32_t &chg, const uint32_t *ex_up,
+                                          const uint32_t *ex_dn, bool use_up, bool use_dn)
+{
+    uint32_t prev_old = 0, up_prev = 0, dn_prev = 0;
+    uint32_t old_j = v[0];
+    uint32_t up_j = __shfl_up_sync(kFull, old_j, 1);
+    uint32_t dn_j = __shfl_down_sync(kFull, old_j, 1);
+    if (use_up) up_j = ex_up[0];
+    if (use_dn) dn_j = ex_dn[0];
+#pragma unroll
+    for (int j = 0; j < S + 2; j++) {
+        uint32_t old_n = 0, up_n = 0, dn_n = 0;
+        if (j + 1 < S + 2) {
+            old_n = v[j + 1];
+            up_n = __shfl_up_sync(kFull, old_n, 1);
+            dn_n = __shfl_down_sync(kFull, old_n, 1);
+            if (use_up) up_n = ex_up[j + 1];
+            if (use_dn) dn_n = ex_dn[j + 1];
+        }
+        uint32_t X[8];
+        X[0] = up_j;
+        X[1] = at_xp1(up_j, up_n);
+        X[2] = at_xp1(old_j, old_n);
+        X[3] = at_xp1(dn_j, dn_n);
+        X[4] = dn_j;
+        X[5] = at_xm1(dn_j, dn_prev);
+        X[6] = at_xm1(old_j, prev_old);
+        X[7] = at_xm1(up_j, up_prev);
+        const uint32_t del = old_j & rule2d<DIR>(X);
+        v[j] = old_j ^ del;
+        if (j >= 1 && j <= S) chg |= del;
+        prev_old = old_j;
+        up_prev = up_j;
+        dn_prev = dn_j;
+        old_j = old_n;
+        up_j = up_n;
+        dn_j = dn_n;
+    }
+}
+
+template <class C, int PH, int I = 0>
+__device__ __forceinline__ void run_subits2d_x(uint32_t (&v)[C::kS + 2], uint32_t &chg, uint32_t *ex, int warp,
+                                               int lane)
+{
+    if constexpr (I < C::kK) {
+        constexpr int S = C::kS, NW = C::kNW, EX = C::EX;
+        // publish this warp's edge rows of the current state (buffer I & 1)
+        uint32_t *buf = ex + (I & 1) * 2 * NW * EX;  // [top rows of NW warps | bottom rows of NW warps]
+        if (lane == 0) {
+#pragma unroll
+            for (int j = 0; j < S + 2; j++) buf[warp * EX + j] = v[j];
+        }
+        if (lane == 31) {
+#pragma unroll
+            for (int j = 0; j < S + 2; j++) buf[(NW + warp) * EX + j] = v[j];
+        }
+        __syncthreads();
+        const bool use_up = lane == 0 && warp > 0, use_dn = lane == 31 && warp < NW - 1;
+        const uint32_t *ex_up = buf + (NW + max(warp - 1, 0)) * EX;  // bottom row of the warp above
+        const uint32_t *ex_dn = buf + min(warp + 1, NW - 1) * EX;    // top row of the warp below
+        subit2d_x<S, (PH + I) & 3>(v, chg, ex_up, ex_dn, use_up, use_dn);
+        run_subits2d_x<C, PH, I + 1>(v, chg, ex, warp, lane);
+    }
+}
+
+template <class C, int PH>
+__device__ bool tile2dx(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar, uint32_t &parity, int *err)
+{
+    constexpr int K = C::kK, S = C::kS, BW = C::BW, BH = C::BH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tx = tile % in.tiles_x, ty = tile / in.tiles_x;
+    const int x0 = tx * S, y0 = ty * C::TH;
+    const CUtensorMap *tm = in.tmap + (q & 1);
+    uint32_t *dst = in.buf[(q + 1) & 1];
+    uint32_t *ex = smem + BW * BH;
+
+    if (threadIdx.x == 0) {
+        tmap_acquire(tm);
+        mbar_arrive_expect_tx(bar, (uint32_t)(BW * BH * 4));
+        tma_load_2d(smem, tm, x0 - 4, y0 - K, bar);
+    }
+    if (!mbar_wait_bounded(bar, parity)) {
+        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
+    }
+    parity ^= 1u;
+
+    const int r = warp * 32 + lane;  // box row of this lane
+    const uint32_t *row = smem + r * BW;
+    uint32_t v[S + 2];
+    v[0] = row[3];
+#pragma unroll
+    for (int c = 0; c < S / 4; c++) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(row + 4 + 4 * c);
+        v[1 + 4 * c] = t.x;
+        v[2 + 4 * c] = t.y;
+        v[3 + 4 * c] = t.z;
+        v[4 + 4 * c] = t.w;
+    }
+    v[S + 1] = row[S + 4];
+
+    uint32_t chg = 0;
+    run_subits2d_x<C, PH>(v, chg, ex, warp, lane);
+
+    const int y = y0 + r - K;  // image row of this lane
+    const bool core = r >= K && r < BH - K && y < in.H;
+    if (core) {
+        uint32_t *drow = dst + (size_t)y * in.P + x0;
+#pragma unroll
+        for (int c = 0; c < S / 4; c++)
+            if (x0 + 4 * c < in.P)
+                *reinterpret_cast<uint4 *>(drow + 4 * c) =
+                    make_uint4(v[1 + 4 * c], v[2 + 4 * c], v[3 + 4 * c], v[4 + 4 * c]);
+    }
+    return __syncthreads_or(core && chg != 0);
+}
+
 // ---------------------------------------------------------------- 3D ------
 template <int NWX, int TZ>
 struct Cfg3D {
