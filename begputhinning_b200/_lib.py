@@ -19,7 +19,7 @@ EXPORTS = [
     "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
     "bgt_batch_reserve", "bgt_batch_reset", "bgt_batch_set_grid",
     "bgt_batch_set_io", "bgt_batch_run", "bgt_batch_instance_stats", "bgt_batch_device_bytes", "bgt_batch_work", "bgt_batch_stage_ms",
-    "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe",
+    "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe", "bgt_rule_table",
     "bgt_server_create", "bgt_server_submit", "bgt_server_poll", "bgt_server_drain", "bgt_server_stats",
     "bgt_server_reset_stats", "bgt_server_destroy",
 ]
@@ -82,6 +82,7 @@ def _declare(L):
         "bgt_tune_get": [I, I, ip],
         "bgt_cfg_list": [I, ip, I, ip],
         "bgt_cfg_describe": [I, ip, ip, ip, ip, ip, ip],
+        "bgt_rule_table": [I, I, vp, vp],
         "bgt_server_create": [I, C.c_size_t, C.POINTER(vp)],
         "bgt_server_submit": [vp, I, vp, I, I, I, vp, C.POINTER(C.c_ulonglong)],
         "bgt_server_poll": [vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_double), ip, I, ip],

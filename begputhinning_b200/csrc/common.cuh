@@ -48,7 +48,7 @@ struct alignas(16) Inst {
     int window;               // passes of constancy that prove a tile fixed (2D)
     uint32_t *buf[2];         // packed ping-pong buffers
     uint32_t *uni;            // 3D pre-test union (per word), null in 2D
-    const CUtensorMap *tmap;  // [2] tensor maps over buf[0], buf[1]
+    const CUtensorMap *tmap;  // [3] tensor maps over buf[0], buf[1], uni (3D)
     int *lc;                  // per-tile pass of the last change (kNever: empty tile)
     uint8_t *act;             // per-tile activity of the current iteration (3D)
     int *list;                // active tile ids of the wave in flight
@@ -125,6 +125,44 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+// Non-blocking probe of phase completion.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Barrier of the 128 threads (warps 0..3) that run tiles (named barrier 1,
+// so a CTA may add warps of other roles that never take part); in 128-thread
+// kernels it is the whole CTA.
+constexpr int kTileThreads = 128;
+__device__ __forceinline__ void tile_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ bool tile_sync_or(bool p)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred a, b;\n\t"
+        "setp.ne.u32 a, %1, 0;\n\t"
+        "bar.red.or.pred b, 1, 128, a;\n\t"
+        "selp.u32 %0, 1, 0, b;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)p)
+        : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ void tmap_acquire(const CUtensorMap *m)
 {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
@@ -175,6 +213,15 @@ __device__ __forceinline__ unsigned long long globaltimer()
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// mbarrier wait bounded by the global timer: false once t_end (ns) passed.
+__device__ __forceinline__ bool mbar_wait_until(uint64_t *bar, uint32_t parity, unsigned long long t_end)
+{
+    for (int i = 0;; i++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 15) == 15 && globaltimer() > t_end) return false;
+    }
 }
 
 }  // namespace bgt

@@ -127,13 +127,15 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
     return fn;
 }
 
-static int encode_map(CUtensorMap *m, const Inst &in, const CfgInfo &c, uint32_t *base)
+// Map over one packed buffer of the instance (`base`: buf[0], buf[1] or the
+// 3D union) with the given box (words, rows, planes).
+static int encode_map(CUtensorMap *m, const Inst &in, const int (&bx)[3], uint32_t *base)
 {
     auto enc = get_encode();
     if (!enc) return fail(BGT_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     cuuint64_t dims[3] = {(cuuint64_t)in.P, (cuuint64_t)in.H, (cuuint64_t)in.D};
     cuuint64_t strides[2] = {(cuuint64_t)in.P * 4, (cuuint64_t)in.P * in.H * 4};
-    cuuint32_t box[3] = {(cuuint32_t)c.box[0], (cuuint32_t)c.box[1], (cuuint32_t)c.box[2]};
+    cuuint32_t box[3] = {(cuuint32_t)bx[0], (cuuint32_t)bx[1], (cuuint32_t)bx[2]};
     cuuint32_t estr[3] = {1, 1, 1};
     const cuuint32_t rank = in.dims == 2 ? 2 : 3;
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT32, rank, base, dims, strides, box, estr,
@@ -287,7 +289,7 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     const size_t off_seq = off; off = align_up(off + (size_t)cap * 4 * 2, 256);
     const size_t off_item = off; off = align_up(off + (size_t)cap * sizeof(int4) * 2, 256);
     const size_t off_inst = off; off = align_up(off + (size_t)N * sizeof(Inst), 256);
-    const size_t off_tmap = off; off = align_up(off + (size_t)N * 2 * sizeof(CUtensorMap), 256);
+    const size_t off_tmap = off; off = align_up(off + (size_t)N * kMapsPerInst * sizeof(CUtensorMap), 256);
     const size_t off_flag = off; off = align_up(off + 64, 256);
     cudaError_t e;
     if (b->reserved) {
@@ -311,7 +313,7 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     b->d_io = (IODesc *)(P + off_io);
     b->cap = cap;
     std::vector<CUtensorMap> &maps = b->maps;
-    maps.assign((size_t)N * 2, CUtensorMap());
+    maps.assign((size_t)N * kMapsPerInst, CUtensorMap());
     for (int i = 0; i < N; i++) {
         Inst &in = b->h[i];
         const Offs &o = offs[i];
@@ -321,10 +323,12 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
         in.lc = (int *)(P + o.lc);
         in.act = (uint8_t *)(P + o.act);
         in.list = (int *)(P + o.list);
-        in.tmap = b->d_tmaps + 2 * i;
+        in.tmap = b->d_tmaps + kMapsPerInst * i;
         const CfgInfo &c = *cfg_info(in.cfg);
-        int rc = encode_map(&maps[2 * i], in, c, in.buf[0]);
-        if (rc == BGT_OK) rc = encode_map(&maps[2 * i + 1], in, c, in.buf[1]);
+        CUtensorMap *m = &maps[(size_t)kMapsPerInst * i];
+        int rc = encode_map(&m[0], in, c.box, in.buf[0]);
+        if (rc == BGT_OK) rc = encode_map(&m[1], in, c.box, in.buf[1]);
+        if (rc == BGT_OK && in.dims == 3) rc = encode_map(&m[2], in, c.ubox, in.uni);
         if (rc != BGT_OK) {
             if (!b->reserved) batch_free_device(b);
             return rc;
@@ -744,6 +748,21 @@ extern "C" int bgt_cfg_describe(int id, int *dims, int *k, int *tw, int *th, int
     if (th) *th = c->TH;
     if (tz) *tz = c->TZc;
     if (smem_bytes) *smem_bytes = c->smem;
+    return BGT_OK;
+}
+
+// Deletable-set table of the device rule of one direction over every
+// neighbourhood (layout in kernels.cu, launch_rule_table): a self-test of the
+// rules against any restatement of the reference's.
+extern "C" int bgt_rule_table(int dims, int dir, uint32_t *d_out, void *stream)
+{
+    if (dims != 2 && dims != 3) return fail(BGT_ERR_ARG, "dims must be 2 or 3");
+    if (dir < 0 || dir >= (dims == 2 ? 4 : 6)) return fail(BGT_ERR_ARG, "direction %d out of range", dir);
+    if (!d_out) return fail(BGT_ERR_ARG, "null output");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = launch_rule_table(dims, dir, d_out, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "rule table");
     return BGT_OK;
 }
 

@@ -25,27 +25,28 @@ using X2_4_28 = Cfg2DX<4, 28, 4>;
 using X2_8_28 = Cfg2DX<8, 28, 4>;
 using C3_8 = Cfg3D<4, 8>;
 using C3_16 = Cfg3D<4, 16>;
-using C3_32 = Cfg3D<4, 32>;
+using C3_4 = Cfg3D<4, 4>;
 
 template <class C>
 constexpr CfgInfo info2d(int id)
 {
-    return CfgInfo{id, 2, C::kK, C::kS, C::kNW, 0, 1, C::kS, C::TH, 1, C::SMEM, {C::BW, C::BH, 1}};
+    return CfgInfo{id, 2, C::kK, C::kS, C::kNW, 0, 1, C::kS, C::TH, 1, C::SMEM, {C::BW, C::BH, 1}, {0, 0, 0}};
 }
 template <class C>
 constexpr CfgInfo info3d(int id)
 {
-    return CfgInfo{id, 3, 1, 0, 0, C::kNWX, C::kTZ, C::kNWX, C::TY, C::kTZ, C::SMEM, {C::BW, C::BH, C::BD}};
+    return CfgInfo{id, 3, 1, 0, 0, C::kNWX, C::kTZ, C::kNWX, C::TY, C::kTZ, C::SMEM, {C::BW, C::BH, C::BD},
+                   {C::kNWX, C::BH, C::kTZ}};
 }
 
 static const CfgInfo kCfgs[] = {
     info2d<C2_1_12>(0), info2d<C2_2_12>(1), info2d<C2_4_12>(2), info2d<C2_8_12>(3),
     info2d<C2_1_28>(4), info2d<C2_2_28>(5), info2d<C2_4_28>(6), info2d<C2_8_28>(7),
     info2d<X2_4_12>(8), info2d<X2_8_12>(9), info2d<X2_16_12>(10), info2d<X2_4_28>(11), info2d<X2_8_28>(12),
-    info3d<C3_8>(16),   info3d<C3_16>(17),  info3d<C3_32>(18),
+    info3d<C3_8>(16),   info3d<C3_16>(17),  info3d<C3_4>(19),
 };
 static const int kIds2d[] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12};
-static const int kIds3d[] = {16, 17, 18};
+static const int kIds3d[] = {19, 16, 17};
 
 const CfgInfo *cfg_info(int id)
 {
@@ -65,36 +66,71 @@ const int *cfg_ids_3d(int *n) { *n = (int)(sizeof(kIds3d) / sizeof(kIds3d[0])); 
 
 constexpr int kThreads = 128;
 
-// Run one tile of instance `in` at pass q with the instance's configuration.
-__device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar, uint32_t &parity,
-                         int *err)
+// Issue the TMA load(s) of one tile of instance `in` for pass q into smem,
+// completing on bar.  One thread calls it, after it has acquired the work
+// item; the proxy fence orders the generic-proxy writes of earlier passes
+// (made visible by that acquire) before the async-proxy reads.
+__device__ void issue_tile(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar)
+{
+    fence_proxy_async_global();
+    switch (in.cfg) {
+#define ISSUE2(ID, C) \
+    case ID: tile2d_issue<C>(in, q, tile, smem, bar); break;
+#define ISSUE3(ID, C) \
+    case ID: tile3d_issue<C>(in, q, tile, smem, bar); break;
+        ISSUE2(0, C2_1_12)
+        ISSUE2(1, C2_2_12)
+        ISSUE2(2, C2_4_12)
+        ISSUE2(3, C2_8_12)
+        ISSUE2(4, C2_1_28)
+        ISSUE2(5, C2_2_28)
+        ISSUE2(6, C2_4_28)
+        ISSUE2(7, C2_8_28)
+        ISSUE2(8, X2_4_12)
+        ISSUE2(9, X2_8_12)
+        ISSUE2(10, X2_16_12)
+        ISSUE2(11, X2_4_28)
+        ISSUE2(12, X2_8_28)
+        ISSUE3(16, C3_8)
+        ISSUE3(17, C3_16)
+        ISSUE3(19, C3_4)
+#undef ISSUE2
+#undef ISSUE3
+    default:
+        break;
+    }
+}
+
+// Run one tile of instance `in` at pass q with the instance's configuration
+// on its box, already in smem.  All tile threads call it.
+__device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem)
 {
     switch (in.cfg) {
-#define CASE2_K1(ID, C)                                                          \
-    case ID:                                                                     \
-        switch (q & 3) {                                                         \
-        case 0: return tile2d<C, 0>(in, q, tile, smem, bar, parity, err);       \
-        case 1: return tile2d<C, 1>(in, q, tile, smem, bar, parity, err);       \
-        case 2: return tile2d<C, 2>(in, q, tile, smem, bar, parity, err);       \
-        default: return tile2d<C, 3>(in, q, tile, smem, bar, parity, err);      \
+#define CASE2_K1(ID, C)                                    \
+    case ID:                                               \
+        switch (q & 3) {                                   \
+        case 0: return tile2d<C, 0>(in, q, tile, smem);   \
+        case 1: return tile2d<C, 1>(in, q, tile, smem);   \
+        case 2: return tile2d<C, 2>(in, q, tile, smem);   \
+        default: return tile2d<C, 3>(in, q, tile, smem);  \
         }
-#define CASE2_K2(ID, C)                                                          \
-    case ID:                                                                     \
-        if (q & 1) return tile2d<C, 2>(in, q, tile, smem, bar, parity, err);    \
-        return tile2d<C, 0>(in, q, tile, smem, bar, parity, err);
+#define CASE2_K2(ID, C)                                         \
+    case ID:                                                    \
+        if (q & 1) return tile2d<C, 2>(in, q, tile, smem);     \
+        return tile2d<C, 0>(in, q, tile, smem);
 #define CASE2_K4(ID, C) \
-    case ID: return tile2d<C, 0>(in, q, tile, smem, bar, parity, err);
+    case ID: return tile2d<C, 0>(in, q, tile, smem);
 #define CASE2X(ID, C) \
-    case ID: return tile2dx<C, 0>(in, q, tile, smem, bar, parity, err);
-#define CASE3(ID, C)                                                             \
-    case ID:                                                                     \
-        switch (q % 6) {                                                         \
-        case 0: return tile3d<C, 0>(in, q, tile, smem, bar, parity, err);       \
-        case 1: return tile3d<C, 1>(in, q, tile, smem, bar, parity, err);       \
-        case 2: return tile3d<C, 2>(in, q, tile, smem, bar, parity, err);       \
-        case 3: return tile3d<C, 3>(in, q, tile, smem, bar, parity, err);       \
-        case 4: return tile3d<C, 4>(in, q, tile, smem, bar, parity, err);       \
-        default: return tile3d<C, 5>(in, q, tile, smem, bar, parity, err);      \
+    case ID: return tile2dx<C, 0>(in, q, tile, smem);
+#define CASE3(ID, C)                                       \
+    case ID:                                               \
+        switch (q % 6) {                                   \
+        case 0: return tile3d<C, 0>(in, q, tile, smem);   \
+        case 1: return tile3d<C, 1>(in, q, tile, smem);   \
+        case 2: return tile3d<C, 2>(in, q, tile, smem);   \
+        case 3: return tile3d<C, 3>(in, q, tile, smem);   \
+        case 4: return tile3d<C, 4>(in, q, tile, smem);   \
+        default: return tile3d<C, 5>(in, q, tile, smem);  \
         }
         CASE2_K1(0, C2_1_12)
         CASE2_K2(1, C2_2_12)
@@ -111,7 +147,7 @@ __device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem, uint64
         CASE2X(12, X2_8_28)
         CASE3(16, C3_8)
         CASE3(17, C3_16)
-        CASE3(18, C3_32)
+        CASE3(19, C3_4)
 #undef CASE2_K1
 #undef CASE2_K2
 #undef CASE2_K4
@@ -120,6 +156,69 @@ __device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem, uint64
     default:
         return false;
     }
+}
+
+// --------------------------------------------------------- rule table -----
+// Deletable sets of the device rules over every neighbourhood, 32 per word:
+// neighbour i (2D: N, NE, E, SE, S, SW, W, NW; 3D: the 26 neighbours in
+// (dz, dy, dx) order, centre skipped) is bit i of the neighbourhood number,
+// whose low 5 bits select the bit of the word.  2D: 8 words per direction,
+// 3D: 2^21 words per direction (centre foreground).
+__device__ __forceinline__ uint32_t lane_pattern(int i)
+{
+    return i == 0 ? 0xAAAAAAAAu : i == 1 ? 0xCCCCCCCCu : i == 2 ? 0xF0F0F0F0u : i == 3 ? 0xFF00FF00u : 0xFFFF0000u;
+}
+
+template <int DIR>
+__global__ void rule2d_table_kernel(uint32_t *out)
+{
+    const int w = threadIdx.x;
+    if (w >= 8) return;
+    uint32_t X[8];
+    for (int i = 0; i < 8; i++) X[i] = i < 5 ? lane_pattern(i) : (((w >> (i - 5)) & 1) ? kFull : 0u);
+    out[w] = rule2d<DIR>(X);
+}
+
+template <int DIR>
+__global__ void rule3d_table_kernel(uint32_t *out)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= (1 << 21)) return;
+    uint32_t g[27];
+    for (int p = 0, i = 0; p < 27; p++) {
+        if (p == 13) {
+            g[p] = kFull;
+            continue;
+        }
+        g[p] = i < 5 ? lane_pattern(i) : (((w >> (i - 5)) & 1) ? kFull : 0u);
+        i++;
+    }
+    out[w] = rule3d<DIR>(g);
+}
+
+cudaError_t launch_rule_table(int dims, int dir, uint32_t *d_out, cudaStream_t st)
+{
+    if (dims == 2) {
+        switch (dir) {
+        case 0: rule2d_table_kernel<0><<<1, 32, 0, st>>>(d_out); break;
+        case 1: rule2d_table_kernel<1><<<1, 32, 0, st>>>(d_out); break;
+        case 2: rule2d_table_kernel<2><<<1, 32, 0, st>>>(d_out); break;
+        case 3: rule2d_table_kernel<3><<<1, 32, 0, st>>>(d_out); break;
+        default: return cudaErrorInvalidValue;
+        }
+    } else {
+        const int grid = (1 << 21) / 256;
+        switch (dir) {
+        case 0: rule3d_table_kernel<0><<<grid, 256, 0, st>>>(d_out); break;
+        case 1: rule3d_table_kernel<1><<<grid, 256, 0, st>>>(d_out); break;
+        case 2: rule3d_table_kernel<2><<<grid, 256, 0, st>>>(d_out); break;
+        case 3: rule3d_table_kernel<3><<<grid, 256, 0, st>>>(d_out); break;
+        case 4: rule3d_table_kernel<4><<<grid, 256, 0, st>>>(d_out); break;
+        case 5: rule3d_table_kernel<5><<<grid, 256, 0, st>>>(d_out); break;
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------ pack --------
@@ -583,8 +682,11 @@ __global__ void __launch_bounds__(kThreads) plain_pass_kernel(Inst *pin, int q, 
     }
     __syncthreads();
     if (!active) return;
-    uint32_t parity = 0;
-    const bool ch = run_tile(in, q, tile, smem, &bar, parity, err);
+    if (threadIdx.x == 0) issue_tile(in, q, tile, smem, &bar);
+    if (!mbar_wait_bounded(&bar, 0)) {
+        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
+    }
+    const bool ch = run_tile(in, q, tile, smem);
     if (threadIdx.x == 0) {
         atomicAdd(&pin->tiles_run, 1ull);
         atomicAdd(&pin->work_words, (unsigned long long)tile_core_words(in, tile));
@@ -610,14 +712,13 @@ cudaError_t launch_plain_pass(int cfg, Inst *d_inst, int ntiles, int q, int *d_f
 }
 
 // ------------------------------------------------------------- engine -----
-// Two work rings (0: critical-path instances first, 1: the rest), each a
-// bounded MPMC queue with per-slot sequence numbers:
+// Two work rings (0: critical-path instances, served first; 1: the rest),
+// each a bounded MPMC queue with per-slot sequence numbers:
 //   seq[s] == t    slot free for ticket t (the producer may write it)
 //   seq[s] == t+1  item of ticket t ready
 //   the consumer of ticket t then sets seq[s] = t + cap.
-// Producers reserve tickets with an atomic on `tail`; consumers claim one by
-// CAS on `head`, only when head < tail, so an idle CTA never commits to a
-// ring it would have to wait on.
+// Producers reserve tickets with an atomic on `tail`; a consumer takes a
+// ticket with one fetch-and-add on `head` when the ring looks non-empty.
 
 __device__ __forceinline__ unsigned ld_acq_u(const unsigned *p)
 {
@@ -637,15 +738,16 @@ __device__ __forceinline__ unsigned ld_volatile_u(const unsigned *p)
 }
 
 // Publish n items (instance ii, tiles list[0..n), pass q) on the instance's
-// ring; item.w carries n so a consumer knows the wave size.  Whole CTA calls.
+// ring; item.w carries n so a consumer knows the wave size.  The tile threads
+// call it.
 __device__ void produce(Sched *S, int ii, int prio, const int *list, int n, int q)
 {
     __shared__ unsigned t0;
     Ring &R = S->ring[prio];
     if (threadIdx.x == 0) t0 = atomicAdd(&R.tail, (unsigned)n);
-    __syncthreads();
+    tile_sync();
     const unsigned cap = R.cap;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = threadIdx.x; i < n; i += kTileThreads) {
         const unsigned t = t0 + (unsigned)i;
         const unsigned s = t % cap;
         bool ok = ld_acq_u(R.seq + s) == t;
@@ -664,13 +766,13 @@ __device__ void produce(Sched *S, int ii, int prio, const int *list, int n, int 
         R.item[s] = make_int4(ii, __ldcg(list + i), q, n);
         st_rel_u(R.seq + s, t + 1);
     }
-    __syncthreads();
+    tile_sync();
 }
 
 // Active tiles of pass q1 (tiles whose 3x3(x3) neighbourhood changed within
 // the window), marked by scattering from the changed tiles into a bitmap in
 // shared memory; falls back to gathering per tile when the instance has more
-// tiles than the bitmap holds.  Whole CTA calls; returns the count.
+// tiles than the bitmap holds.  The tile threads call it; returns the count.
 __device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int scratch_words)
 {
     __shared__ int cnt;
@@ -680,10 +782,10 @@ __device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int s
     const int thr = q1 - window;
     if (2 * nwords <= scratch_words) {
         uint32_t *act = scratch, *ne = scratch + nwords;
-        for (int i = threadIdx.x; i < 2 * nwords; i += blockDim.x) scratch[i] = 0;
-        __syncthreads();
+        for (int i = threadIdx.x; i < 2 * nwords; i += kTileThreads) scratch[i] = 0;
+        tile_sync();
         const int tx = in.tiles_x, ty = in.tiles_y, tz = in.tiles_z;
-        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        for (int t = threadIdx.x; t < nt; t += kTileThreads) {
             const int v = ld_cg_int(in.lc + t);
             if (v == kNever) continue;
             atomicOr(ne + (t >> 5), 1u << (t & 31));
@@ -704,8 +806,8 @@ __device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int s
                 }
             }
         }
-        __syncthreads();
-        for (int w = threadIdx.x; w < nwords; w += blockDim.x) {
+        tile_sync();
+        for (int w = threadIdx.x; w < nwords; w += kTileThreads) {
             uint32_t m = act[w] & ne[w];
             while (m) {
                 const int b = __ffs(m) - 1;
@@ -714,16 +816,16 @@ __device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int s
             }
         }
     } else {
-        __syncthreads();
-        for (int t = threadIdx.x; t < nt; t += blockDim.x)
+        tile_sync();
+        for (int t = threadIdx.x; t < nt; t += kTileThreads)
             if (ld_cg_int(in.lc + t) != kNever && nbr_last_change(in, t) >= thr) in.list[atomicAdd(&cnt, 1)] = t;
     }
-    __syncthreads();
+    tile_sync();
     return cnt;
 }
 
 // Build the active list for pass q1 of instance ii and publish it, or retire
-// the instance.  Whole CTA calls.  3D instances rebuild the list only at
+// the instance.  The tile threads call it.  3D instances rebuild the list only at
 // iteration starts (the union pass decides activity for the iteration).
 __device__ void next_wave(Sched *S, Inst *insts, int ii, int q1, int nprev, uint32_t *scratch, int scratch_words)
 {
@@ -753,7 +855,7 @@ __device__ void next_wave(Sched *S, Inst *insts, int ii, int q1, int nprev, uint
         }
         cnt = retire ? 0 : n;
     }
-    __syncthreads();
+    tile_sync();
     const int m = cnt;
     if (m > 0) produce(S, ii, in.prio, in.list, m, q1);
 }
@@ -811,7 +913,11 @@ __device__ __forceinline__ int wait_ticket(Sched *S, int r, unsigned t, int4 &ou
     }
 }
 
-__global__ void __launch_bounds__(kThreads) engine_kernel(Inst *insts, Sched *S, int scratch_words)
+// Persistent engine: thread 0 of each CTA claims a work item (ring 0 first),
+// stages the tile by TMA; the CTA computes it, records its change, counts it
+// against its wave and, for the wave's last tile, builds and publishes the
+// instance's next wave.  Every wait is bounded and reports a status bit.
+__global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched *S, int scratch_words)
 {
     extern __shared__ __align__(128) uint32_t smem_raw[];
     uint32_t *smem = align128(smem_raw);
@@ -843,6 +949,7 @@ __global__ void __launch_bounds__(kThreads) engine_kernel(Inst *insts, Sched *S,
                     if (w == 0) continue;  // abandoned: that ring is finished
                     item = it;
                     g = 1;
+                    issue_tile(insts[it.x], it.z, it.y, smem, &bar);
                     break;
                 }
                 if (ld_acquire(&S->live) == 0) break;
@@ -858,8 +965,11 @@ __global__ void __launch_bounds__(kThreads) engine_kernel(Inst *insts, Sched *S,
         if (!got) break;
         const int ii = item.x, tile = item.y, q = item.z, nwave = item.w;
         Inst &in = insts[ii];
-        fence_proxy_async_global();
-        const bool ch = run_tile(in, q, tile, smem, &bar, parity, &S->status);
+        if (!mbar_wait_bounded(&bar, parity)) {
+            if (threadIdx.x == 0) atomicOr(&S->status, kErrTmaTimeout);
+        }
+        parity ^= 1u;
+        const bool ch = run_tile(in, q, tile, smem);  // ends with a barrier: smem is free again
         if (threadIdx.x == 0) {
             if (ch) in.lc[tile] = q;
             __threadfence();

@@ -9,15 +9,19 @@
 
 namespace bgt {
 
-// Tile configurations.  2D ids 0..7: (K, S) with NW = 4 warps; 3D ids 16..18:
-// (NWX = 4, TZ).  All use 128 threads so the persistent engine can run any
-// mix of them in one launch.
+// Tile configurations.  2D ids 0..7: (K, S) with NW = 4 warps, ids 8..12 the
+// same with shared warp edges; 3D ids 16, 17, 19: (NWX = 4, TZ = 8, 16, 4).
+// All use 128 threads so the persistent engine can run any mix of them in
+// one launch.
 struct CfgInfo {
     int id, dims, k, S, NW, NWX, TZ;
     int TW, TH, TZc;  // core tile extent (words, rows, planes)
     int smem;         // dynamic shared memory bytes
     int box[3];       // TMA box (words, rows, planes)
+    int ubox[3];      // TMA box of the 3D union (core words, rows, core planes)
 };
+// Tensor maps per instance: buf[0], buf[1] and (3D) the union.
+constexpr int kMapsPerInst = 3;
 const CfgInfo *cfg_info(int id);  // nullptr if unknown
 int max_cfg_smem();               // largest dynamic shared memory of any configuration
 const int *cfg_ids_2d(int *n);
@@ -68,6 +72,7 @@ cudaError_t launch_tile_init(const Inst *d_inst, const Inst &h_inst, int *d_coun
 cudaError_t launch_plain_pass(int cfg, Inst *d_inst, int ntiles, int q, int *d_flag, int *d_err,
                               cudaStream_t st);
 cudaError_t launch_engine(int grid, int smem, Inst *d_insts, int ninst, Sched *d_sched, cudaStream_t st);
+cudaError_t launch_rule_table(int dims, int dir, uint32_t *d_out, cudaStream_t st);
 int engine_max_blocks_per_sm(int smem);
 cudaError_t engine_set_smem(int smem);
 

@@ -20,15 +20,24 @@ namespace bgt {
 // ---------------------------------------------------------------- 2D ------
 // x0..x7 = neighbours clockwise N, NE, E, SE, S, SW, W, NW after rotation;
 // returns the mask of centre bits that are deletable (before & centre).
+//
+// The reference writes the rule as a sum of five products
+//   a = ~x1 ~x7 (x2^x3^~x4)(x3^x5)(x3^x6),  b = x2 x4 (x6|~x7),  c = ~x1 x4 x6,
+//   d = ~x6 ~x7 (x1^x5)(x2^x5)(x4^~x5),     e = ~x1 ~x2 ~x3 x6 x7.
+// Here it is factored by the context (x5, x6, x7) into fewer three-input
+// operations; the two forms agree on all 256 neighbourhoods:
+//   x6 | x5 ~x7          ->  H  = x4 (x2 | ~x1)
+//   x6 (x5 | x7)         ->  also Z = no foreground among x1..x4
+//   ~x5 ~x6 ~x7          ->  G0 = x2 (x1|x3|x4) | ~x1 ~x2 x3 x4
 __device__ __forceinline__ uint32_t north_template(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3,
                                                    uint32_t x4, uint32_t x5, uint32_t x6, uint32_t x7)
 {
-    const uint32_t a = ~x1 & ~x7 & (x2 ^ x3 ^ ~x4) & (x3 ^ x5) & (x3 ^ x6);
-    const uint32_t b = x2 & x4 & (x6 | ~x7);
-    const uint32_t c = ~x1 & x4 & x6;
-    const uint32_t d = ~x6 & ~x7 & (x1 ^ x5) & (x2 ^ x5) & (x4 ^ ~x5);
-    const uint32_t e = ~x1 & ~x2 & ~x3 & x6 & x7;
-    return ~x0 & (a | b | c | d | e);
+    const uint32_t h = x4 & (x2 | ~x1);
+    const uint32_t c1 = x6 | (x5 & ~x7);
+    const uint32_t z = x6 & (x5 | x7) & ~(x1 | x2 | x3 | x4);
+    const uint32_t g0 = (x2 & (x1 | x3 | x4)) | (~x1 & ~x2 & x3 & x4);
+    const uint32_t c3 = ~(x5 | x6 | x7);
+    return ~x0 & ((c1 & h) | z | (c3 & g0));
 }
 
 // Direction s in application order 0..3 = N, S, E, W -> ring rotation.

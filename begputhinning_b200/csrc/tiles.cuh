@@ -4,11 +4,13 @@
 // 2D tile, configuration (K, S, NW): a CTA of NW warps.  Warp w owns 32
 // consecutive rows, one row per lane; the lane holds S+2 words of its row in
 // registers (S core words plus one halo word each side).  K subiterations run
-// on those registers: y-neighbours come from the lanes above/below through
-// warp shuffles, x-neighbours from the adjacent registers through funnel
-// shifts.  Lanes 0..K-1 and 32-K..31 are halo rows (their state is only
-// valid for the lanes inside them), so a warp keeps 32-2K core rows and
-// consecutive warps overlap by 2K rows.  The tile (core plus halo) is staged
+// on those registers: a lane forms the x-neighbours of its own row by funnel
+// shifts of adjacent registers (two per word) and receives the three words
+// of the row above and of the row below (centre, x+1, x-1) by warp shuffles,
+// which keeps the integer pipe for the rule itself.  Lanes 0..K-1 and
+// 32-K..31 are halo rows (their state is only valid for the lanes inside
+// them), so a warp keeps 32-2K core rows and consecutive warps overlap by 2K
+// rows.  The tile (core plus halo) is staged
 // into shared memory by one TMA load; out-of-image parts read as zero.
 //
 // 3D tile, configuration (NWX, TZ): one subiteration per pass.  Warp w owns
@@ -29,36 +31,25 @@ namespace bgt {
 template <int S, int DIR>
 __device__ __forceinline__ void subit2d(uint32_t (&v)[S + 2], uint32_t &chg)
 {
-    uint32_t prev_old = 0, up_prev = 0, dn_prev = 0;
-    uint32_t old_j = v[0];
-    uint32_t up_j = __shfl_up_sync(kFull, old_j, 1);
-    uint32_t dn_j = __shfl_down_sync(kFull, old_j, 1);
+    uint32_t prev_old = 0;
 #pragma unroll
     for (int j = 0; j < S + 2; j++) {
-        uint32_t old_n = 0, up_n = 0, dn_n = 0;
-        if (j + 1 < S + 2) {
-            old_n = v[j + 1];
-            up_n = __shfl_up_sync(kFull, old_n, 1);
-            dn_n = __shfl_down_sync(kFull, old_n, 1);
-        }
+        const uint32_t old_j = v[j];
+        const uint32_t old_n = j + 1 < S + 2 ? v[j + 1] : 0u;
+        const uint32_t xp = at_xp1(old_j, old_n), xm = at_xm1(old_j, prev_old);
         uint32_t X[8];
-        X[0] = up_j;
-        X[1] = at_xp1(up_j, up_n);
-        X[2] = at_xp1(old_j, old_n);
-        X[3] = at_xp1(dn_j, dn_n);
-        X[4] = dn_j;
-        X[5] = at_xm1(dn_j, dn_prev);
-        X[6] = at_xm1(old_j, prev_old);
-        X[7] = at_xm1(up_j, up_prev);
+        X[0] = __shfl_up_sync(kFull, old_j, 1);
+        X[1] = __shfl_up_sync(kFull, xp, 1);
+        X[7] = __shfl_up_sync(kFull, xm, 1);
+        X[4] = __shfl_down_sync(kFull, old_j, 1);
+        X[3] = __shfl_down_sync(kFull, xp, 1);
+        X[5] = __shfl_down_sync(kFull, xm, 1);
+        X[2] = xp;
+        X[6] = xm;
         const uint32_t del = old_j & rule2d<DIR>(X);
         v[j] = old_j ^ del;
         if (j >= 1 && j <= S) chg |= del;
         prev_old = old_j;
-        up_prev = up_j;
-        dn_prev = dn_j;
-        old_j = old_n;
-        up_j = up_n;
-        dn_j = dn_n;
     }
 }
 
@@ -84,28 +75,29 @@ struct Cfg2D {
     static_assert(BW <= 256 && BH <= 256, "TMA box too large");
 };
 
-// Process one 2D tile for pass q (phase PH = first direction of the pass).
-// Returns (to all threads) whether any core pixel was deleted.
-template <class C, int PH>
-__device__ bool tile2d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar, uint32_t &parity,
-                       int *err)
+// Issue the TMA load of the box of a 2D tile (core plus halo) for pass q
+// into smem; completes on bar.  One thread calls it.  Serves Cfg2D and Cfg2DX.
+template <class C>
+__device__ __forceinline__ void tile2d_issue(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar)
 {
-    constexpr int K = C::kK, S = C::kS, CORE = C::CORE, BW = C::BW, BH = C::BH;
+    const int tx = tile % in.tiles_x, ty = tile / in.tiles_x;
+    const CUtensorMap *tm = in.tmap + (q & 1);
+    tmap_acquire(tm);
+    mbar_arrive_expect_tx(bar, (uint32_t)(C::BW * C::BH * 4));
+    tma_load_2d(smem, tm, tx * C::kS - 4, ty * C::TH - C::kK, bar);
+}
+
+// Process one 2D tile for pass q (phase PH = first direction of the pass)
+// from its box in smem.  Returns (to all tile threads) whether any core
+// pixel was deleted.
+template <class C, int PH>
+__device__ bool tile2d(const Inst &in, int q, int tile, const uint32_t *smem)
+{
+    constexpr int K = C::kK, S = C::kS, CORE = C::CORE, BW = C::BW;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tx = tile % in.tiles_x, ty = tile / in.tiles_x;
     const int x0 = tx * S, y0 = ty * C::TH;
-    const CUtensorMap *tm = in.tmap + (q & 1);
     uint32_t *dst = in.buf[(q + 1) & 1];
-
-    if (threadIdx.x == 0) {
-        tmap_acquire(tm);
-        mbar_arrive_expect_tx(bar, (uint32_t)C::SMEM);
-        tma_load_2d(smem, tm, x0 - 4, y0 - K, bar);
-    }
-    if (!mbar_wait_bounded(bar, parity)) {
-        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
-    }
-    parity ^= 1u;
 
     const int r = warp * CORE + lane;  // box row of this lane
     const uint32_t *row = smem + r * BW;
@@ -134,9 +126,7 @@ __device__ bool tile2d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t
                 *reinterpret_cast<uint4 *>(drow + 4 * c) =
                     make_uint4(v[1 + 4 * c], v[2 + 4 * c], v[3 + 4 * c], v[4 + 4 * c]);
     }
-    const bool any = __syncthreads_or(core && chg != 0);  // also frees smem for the next tile
-    (void)BH;
-    return any;
+    return tile_sync_or(core && chg != 0);
 }
 
 // ------------------------------------------- 2D, shared warp edges -------
@@ -217,7 +207,7 @@ __device__ __forceinline__ void run_subits2d_x(uint32_t (&v)[C::kS + 2], uint32_
 #pragma unroll
             for (int j = 0; j < S + 2; j++) buf[(NW + warp) * EX + j] = v[j];
         }
-        __syncthreads();
+        tile_sync();
         const bool use_up = lane == 0 && warp > 0, use_dn = lane == 31 && warp < NW - 1;
         const uint32_t *ex_up = buf + (NW + max(warp - 1, 0)) * EX;  // bottom row of the warp above
         const uint32_t *ex_dn = buf + min(warp + 1, NW - 1) * EX;    // top row of the warp below
@@ -227,25 +217,14 @@ __device__ __forceinline__ void run_subits2d_x(uint32_t (&v)[C::kS + 2], uint32_
 }
 
 template <class C, int PH>
-__device__ bool tile2dx(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar, uint32_t &parity, int *err)
+__device__ bool tile2dx(const Inst &in, int q, int tile, uint32_t *smem)
 {
     constexpr int K = C::kK, S = C::kS, BW = C::BW, BH = C::BH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tx = tile % in.tiles_x, ty = tile / in.tiles_x;
     const int x0 = tx * S, y0 = ty * C::TH;
-    const CUtensorMap *tm = in.tmap + (q & 1);
     uint32_t *dst = in.buf[(q + 1) & 1];
     uint32_t *ex = smem + BW * BH;
-
-    if (threadIdx.x == 0) {
-        tmap_acquire(tm);
-        mbar_arrive_expect_tx(bar, (uint32_t)(BW * BH * 4));
-        tma_load_2d(smem, tm, x0 - 4, y0 - K, bar);
-    }
-    if (!mbar_wait_bounded(bar, parity)) {
-        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
-    }
-    parity ^= 1u;
 
     const int r = warp * 32 + lane;  // box row of this lane
     const uint32_t *row = smem + r * BW;
@@ -274,7 +253,7 @@ __device__ bool tile2dx(const Inst &in, int q, int tile, uint32_t *smem, uint64_
                 *reinterpret_cast<uint4 *>(drow + 4 * c) =
                     make_uint4(v[1 + 4 * c], v[2 + 4 * c], v[3 + 4 * c], v[4 + 4 * c]);
     }
-    return __syncthreads_or(core && chg != 0);
+    return tile_sync_or(core && chg != 0);
 }
 
 // ---------------------------------------------------------------- 3D ------
@@ -285,7 +264,9 @@ struct Cfg3D {
     static constexpr int BW = NWX + 8;        // box width in words
     static constexpr int BH = 32;             // box rows
     static constexpr int BD = TZ + 2;         // box planes
-    static constexpr int SMEM = BW * BH * BD * 4;
+    static constexpr int IMG = BW * BH * BD * 4;  // bytes of the image box
+    static constexpr int UNI = NWX * BH * TZ * 4; // bytes of the union box (core words and planes)
+    static constexpr int SMEM = IMG + UNI;
     static constexpr int THREADS = NWX * 32;
     static_assert(NWX % 4 == 0, "NWX must be a multiple of 4 (TMA x alignment)");
     static_assert(BD <= 256, "TMA box too large");
@@ -303,10 +284,31 @@ __device__ __forceinline__ void plane3x3(const uint32_t *p, int col, uint32_t (&
     o[6] = at_xm1(cd, ld); o[7] = cd; o[8] = at_xp1(cd, rd);
 }
 
+// Issue the TMA loads of a 3D tile for pass q: the image box (core plus
+// one halo word/row/plane) and, in passes 1..5 of an iteration, the union
+// box behind it.  One thread calls it.
+template <class C>
+__device__ __forceinline__ void tile3d_issue(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar)
+{
+    const int tx = tile % in.tiles_x;
+    const int ty = (tile / in.tiles_x) % in.tiles_y;
+    const int tz = tile / (in.tiles_x * in.tiles_y);
+    const int x0 = tx * C::kNWX, y0 = ty * C::TY, z0 = tz * C::kTZ;
+    const CUtensorMap *tm = in.tmap + (q & 1);
+    tmap_acquire(tm);
+    if (q % 6 == 0) {
+        mbar_arrive_expect_tx(bar, (uint32_t)C::IMG);
+    } else {
+        tmap_acquire(in.tmap + 2);
+        mbar_arrive_expect_tx(bar, (uint32_t)(C::IMG + C::UNI));
+        tma_load_3d(smem + C::IMG / 4, in.tmap + 2, x0, y0 - 1, z0, bar);
+    }
+    tma_load_3d(smem, tm, x0 - 4, y0 - 1, z0 - 1, bar);
+}
+
 // MODE 0: pre-test union (stored) + U.  MODE 1..5: N, E, D, S, W.
 template <class C, int MODE>
-__device__ bool tile3d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t *bar, uint32_t &parity,
-                       int *err)
+__device__ bool tile3d(const Inst &in, int q, int tile, const uint32_t *smem)
 {
     constexpr int NWX = C::kNWX, TZ = C::kTZ, BW = C::BW, BH = C::BH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -314,18 +316,8 @@ __device__ bool tile3d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t
     const int ty = (tile / in.tiles_x) % in.tiles_y;
     const int tz = tile / (in.tiles_x * in.tiles_y);
     const int x0 = tx * NWX, y0 = ty * C::TY, z0 = tz * TZ;
-    const CUtensorMap *tm = in.tmap + (q & 1);
     uint32_t *dst = in.buf[(q + 1) & 1];
-
-    if (threadIdx.x == 0) {
-        tmap_acquire(tm);
-        mbar_arrive_expect_tx(bar, (uint32_t)C::SMEM);
-        tma_load_3d(smem, tm, x0 - 4, y0 - 1, z0 - 1, bar);
-    }
-    if (!mbar_wait_bounded(bar, parity)) {
-        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
-    }
-    parity ^= 1u;
+    const uint32_t *usm = smem + C::IMG / 4;  // union box: [plane][row][word]
 
     const int col = 4 + warp;
     const int x = x0 + warp, y = y0 + lane - 1;
@@ -361,7 +353,7 @@ __device__ bool tile3d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t
                 if (live) in.uni[idx] = un & val;
                 del = val & du;
             } else {
-                const uint32_t un = live ? ld_cg(in.uni + idx) : 0u;
+                const uint32_t un = usm[(zz * BH + lane) * NWX + warp];
                 del = val & rule3d<MODE>(g) & un;
             }
             nv = val & ~del;
@@ -374,10 +366,9 @@ __device__ bool tile3d(const Inst &in, int q, int tile, uint32_t *smem, uint64_t
             B[i] = Cn[i];
         }
     }
-    (void)NWX;
     // the barrier orders every thread's stores before thread 0's fence and
     // release (engine) or the end of the launch (plain path)
-    return __syncthreads_or(chg != 0u);
+    return tile_sync_or(chg != 0u);
 }
 
 // ------------------------------------------------------------ activity ----

@@ -192,6 +192,15 @@ int bgt_cfg_list(int dims, int *ids, int cap, int *n);
 /* k = subiterations per pass, tw/th/tz = core tile extent (words, rows, planes) */
 int bgt_cfg_describe(int id, int *dims, int *k, int *tw, int *th, int *tz, int *smem_bytes);
 
+/* Self-test of the device rules (no reference counterpart): the deletable
+ * set of direction dir (2D 0..3 = N,S,E,W; 3D 0..5 = U,N,E,D,S,W) over every
+ * neighbourhood of a foreground centre, 32 neighbourhoods per word.
+ * Neighbour i (2D: N,NE,E,SE,S,SW,W,NW; 3D: the 26 neighbours in (dz,dy,dx)
+ * order, centre skipped) is bit i of the neighbourhood number n; n lives in
+ * bit n%32 of word n/32.  d_out: 8 words (2D) or 2^21 words (3D) of device
+ * memory.  Synchronises the stream. */
+int bgt_rule_table(int dims, int dir, uint32_t *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

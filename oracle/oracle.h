@@ -92,6 +92,13 @@ uint64_t oracle_rule3d(int dir, const uint64_t *nb);
 typedef unsigned int (*ref_rule3d_fn)(int dir, unsigned int val, unsigned int *n26, unsigned int prev);
 long long oracle_rule3d_exhaustive(int dir, ref_rule3d_fn ref);
 
+/* Deletable-set table of a direction over every neighbourhood of a
+ * foreground centre: neighbour i (2D: N,NE,E,SE,S,SW,W,NW; 3D: the 26
+ * neighbours in (dz,dy,dx) order, centre skipped) is bit i of the
+ * neighbourhood number n, n in bit n%32 of word n/32.  2D: 8 words, 3D:
+ * 2^21 words. */
+void oracle_rule_table(int dims, int dir, uint32_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,6 +110,7 @@ def lib():
         L.oracle_prune_smooth.argtypes = [C.POINTER(_Segs), C.c_int, C.c_int, C.c_int, C.POINTER(_CL)]
         L.oracle_cl_free.argtypes = [C.POINTER(_CL)]
         L.oracle_binarise.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_int, u8p]
+        L.oracle_rule_table.argtypes = [C.c_int, C.c_int, C.c_void_p]
         L.oracle_rule2d.argtypes = [C.c_int, C.POINTER(C.c_uint64)]
         L.oracle_rule2d.restype = C.c_uint64
         L.oracle_rule3d.argtypes = [C.c_int, C.POINTER(C.c_uint64)]
@@ -233,6 +234,14 @@ def rule2d(direction: int, x8: np.ndarray) -> np.ndarray:
 def rule3d(direction: int, nb27: np.ndarray) -> np.ndarray:
     a = np.ascontiguousarray(nb27, np.uint64)
     return np.uint64(lib().oracle_rule3d(direction, a.ctypes.data_as(C.POINTER(C.c_uint64))))
+
+
+def rule_table(dims: int, direction: int) -> np.ndarray:
+    """Deletable-set table of one direction over every neighbourhood
+    (uint32[8] in 2D, uint32[2^21] in 3D; layout of bgt_rule_table)."""
+    out = np.zeros(8 if dims == 2 else 1 << 21, np.uint32)
+    lib().oracle_rule_table(dims, direction, out.ctypes.data_as(C.c_void_p))
+    return out
 
 
 def rule3d_exhaustive_vs_ref(direction: int) -> int:

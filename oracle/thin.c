@@ -240,6 +240,43 @@ long long oracle_rule3d_exhaustive(int dir, ref_rule3d_fn ref)
     return bad;
 }
 
+/* Deletable-set table of direction dir over every neighbourhood of a
+ * foreground centre, in the layout of the device self-test (bgt_rule_table):
+ * neighbour i is bit i of the neighbourhood number n, n in bit n%32 of word
+ * n/32.  2D: 8 words, 3D: 2^21 words. */
+void oracle_rule_table(int dims, int dir, uint32_t *out)
+{
+    unsigned int lane_pat[5];
+    for (int i = 0; i < 5; i++) {
+        unsigned int w = 0;
+        for (int l = 0; l < 32; l++)
+            if ((l >> i) & 1) w |= 1u << l;
+        lane_pat[i] = w;
+    }
+    if (dims == 2) {
+        for (uint32_t hi = 0; hi < 8; hi++) {
+            uint64_t X[8];
+            for (int i = 0; i < 8; i++) X[i] = i < 5 ? lane_pat[i] : (((hi >> (i - 5)) & 1) ? 0xffffffffu : 0u);
+            out[hi] = (uint32_t)oracle_rule2d(dir, X);
+        }
+        return;
+    }
+    build_frames();
+    for (uint32_t hi = 0; hi < (1u << 21); hi++) {
+        w64 g[27], loc[27];
+        for (int p = 0, i = 0; p < 27; p++) {
+            if (p == 13) {
+                g[p] = 0xffffffffu;
+                continue;
+            }
+            g[p] = i < 5 ? lane_pat[i] : (((hi >> (i - 5)) & 1) ? 0xffffffffu : 0u);
+            i++;
+        }
+        for (int i = 0; i < 27; i++) loc[i] = g[frame_map[dir][i]];
+        out[hi] = (uint32_t)up_template(loc);
+    }
+}
+
 int oracle_thin3d(uint8_t *vol, int w, int h, int d, int nthreads)
 {
     if (w <= 0 || h <= 0 || d <= 0) return 0;
