@@ -10,8 +10,8 @@
 // which keeps the integer pipe for the rule itself.  Lanes 0..K-1 and
 // 32-K..31 are halo rows (their state is only valid for the lanes inside
 // them), so a warp keeps 32-2K core rows and consecutive warps overlap by 2K
-// rows.  The tile (core plus halo) is staged
-// into shared memory by one TMA load; out-of-image parts read as zero.
+// rows.  The tile (core plus halo) is staged into shared memory by one TMA
+// load; out-of-image parts read as zero.
 //
 // 3D tile, configuration (NWX, TZ): one subiteration per pass.  Warp w owns
 // word column x0+w; its lanes are 32 consecutive rows (30 core rows and one
@@ -28,37 +28,39 @@
 namespace bgt {
 
 // ---------------------------------------------------------------- 2D ------
+// One subiteration on the lane's S+2 words.  Word steps whose centre words
+// are empty in every lane of the warp are skipped (nothing to delete there).
 template <int S, int DIR>
-__device__ __forceinline__ void subit2d(uint32_t (&v)[S + 2], uint32_t &chg)
+__device__ __forceinline__ void subit2d(uint32_t (&v)[S + 2])
 {
     uint32_t prev_old = 0;
 #pragma unroll
     for (int j = 0; j < S + 2; j++) {
         const uint32_t old_j = v[j];
-        const uint32_t old_n = j + 1 < S + 2 ? v[j + 1] : 0u;
-        const uint32_t xp = at_xp1(old_j, old_n), xm = at_xm1(old_j, prev_old);
-        uint32_t X[8];
-        X[0] = __shfl_up_sync(kFull, old_j, 1);
-        X[1] = __shfl_up_sync(kFull, xp, 1);
-        X[7] = __shfl_up_sync(kFull, xm, 1);
-        X[4] = __shfl_down_sync(kFull, old_j, 1);
-        X[3] = __shfl_down_sync(kFull, xp, 1);
-        X[5] = __shfl_down_sync(kFull, xm, 1);
-        X[2] = xp;
-        X[6] = xm;
-        const uint32_t del = old_j & rule2d<DIR>(X);
-        v[j] = old_j ^ del;
-        if (j >= 1 && j <= S) chg |= del;
+        if (__any_sync(kFull, old_j != 0u)) {
+            const uint32_t old_n = j + 1 < S + 2 ? v[j + 1] : 0u;
+            const uint32_t xp = at_xp1(old_j, old_n), xm = at_xm1(old_j, prev_old);
+            uint32_t X[8];
+            X[0] = __shfl_up_sync(kFull, old_j, 1);
+            X[1] = __shfl_up_sync(kFull, xp, 1);
+            X[7] = __shfl_up_sync(kFull, xm, 1);
+            X[4] = __shfl_down_sync(kFull, old_j, 1);
+            X[3] = __shfl_down_sync(kFull, xp, 1);
+            X[5] = __shfl_down_sync(kFull, xm, 1);
+            X[2] = xp;
+            X[6] = xm;
+            v[j] = old_j & ~rule2d<DIR>(X);
+        }
         prev_old = old_j;
     }
 }
 
 template <int K, int S, int PH, int I = 0>
-__device__ __forceinline__ void run_subits2d(uint32_t (&v)[S + 2], uint32_t &chg)
+__device__ __forceinline__ void run_subits2d(uint32_t (&v)[S + 2])
 {
     if constexpr (I < K) {
-        subit2d<S, (PH + I) & 3>(v, chg);
-        run_subits2d<K, S, PH, I + 1>(v, chg);
+        subit2d<S, (PH + I) & 3>(v);
+        run_subits2d<K, S, PH, I + 1>(v);
     }
 }
 
@@ -113,9 +115,13 @@ __device__ bool tile2d(const Inst &in, int q, int tile, const uint32_t *smem)
     }
     v[S + 1] = row[S + 4];
 
-    uint32_t chg = 0;
-    run_subits2d<K, S, PH>(v, chg);
+    run_subits2d<K, S, PH>(v);
 
+    // change of the core words over the pass: the box in smem still holds
+    // the pass's input
+    uint32_t chg = 0;
+#pragma unroll
+    for (int c = 0; c < S; c++) chg |= v[1 + c] ^ row[4 + c];
     const int y = y0 + r - K;  // image row of this lane
     const bool core = lane >= K && lane < 32 - K && y < in.H;
     if (core) {
