@@ -107,68 +107,159 @@ extern "C" int bgt_segments3d_device(bgt_ctx *c, int dtype, const void *d_vol, i
 }
 
 // ------------------------------------------------------------ centerline --
-// Pruning, smoothing and CSR flattening, operation for operation as
-// 2D/CenterlineExtraction.cpp:51-131 and 3D/CenterlineExtraction.cpp:56-144
-// (a float running sum to which the integer coordinates are added and from
-// which they are subtracted one at a time, divided by float(n)), so the float
-// outputs are bit-identical.  A negative smoothing_span is treated as 0 (the
-// reference indexes out of bounds there).
-static int prune_smooth(const HostSegs &s, int dims, int max_segment_length, int smoothing_span, float **ox,
-                        float **oy, float **oz, unsigned int **oidx, unsigned int *nsegs_out)
+// Pruning, smoothing and CSR flattening on the device, operation for
+// operation as 2D/CenterlineExtraction.cpp:51-131 and
+// 3D/CenterlineExtraction.cpp:56-144:
+//  * a segment is kept when (size_t)n > (size_t)max_segment_length or it is
+//    not an end segment;
+//  * kept segments are renumbered in order (prefix sums of the keep flags
+//    and of the kept point counts give each one its CSR slot);
+//  * each kept segment is smoothed by one thread with the reference's float
+//    running sum (integer coordinates added to and subtracted from it one at
+//    a time, IEEE round-to-nearest adds and divide by float(count)), so the
+//    float outputs are bit-identical.  A negative smoothing_span is treated
+//    as 0 (the reference indexes out of bounds there).
+__global__ void prune_flags_kernel(const int32_t *__restrict__ start, const uint8_t *__restrict__ is_end, int S,
+                                   unsigned long long maxlen, int *keep, int *kpts)
 {
-    const size_t maxlen = (size_t)(long long)max_segment_length;  // size_t comparison as in the reference
-    unsigned nsegs = 0, npts = 0;
-    for (int k = 0; k < s.nseg; k++) {
-        const size_t n = (size_t)(s.start[k + 1] - s.start[k]);
-        if ((n > maxlen) || !s.is_end[k]) {
-            nsegs++;
-            npts += (unsigned)n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+        const long long n = (long long)start[k + 1] - start[k];
+        const bool kp = (unsigned long long)n > maxlen || !is_end[k];
+        keep[k] = kp ? 1 : 0;
+        kpts[k] = kp ? (int)n : 0;
+    }
+}
+
+template <bool Z3>
+__global__ void smooth_kernel(const int32_t *__restrict__ start, const int16_t *__restrict__ px,
+                              const int16_t *__restrict__ py, const int16_t *__restrict__ pz,
+                              const int *__restrict__ keep, const int *__restrict__ seg_new,
+                              const int *__restrict__ pt_new, int S, int span_req, float *X, float *Y, float *Zo,
+                              unsigned *I)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+        if (!keep[k]) continue;
+        const int b = start[k], n = start[k + 1] - b;
+        int pi = pt_new[k];
+        I[seg_new[k]] = (unsigned)pi;
+        const int16_t *sx = px + b, *sy = py + b, *sz = Z3 ? pz + b : nullptr;
+        const int span = min(span_req, (n - 1) / 2);
+        float x = sx[0], y = sy[0], z = Z3 ? (float)sz[0] : 0.f;
+        int cnt = 1;
+        X[pi] = (float)sx[0];
+        Y[pi] = (float)sy[0];
+        if (Z3) Zo[pi] = (float)sz[0];
+        pi++;
+        auto add = [&](int q) {
+            x = __fadd_rn(x, (float)sx[q]);
+            y = __fadd_rn(y, (float)sy[q]);
+            if (Z3) z = __fadd_rn(z, (float)sz[q]);
+        };
+        auto sub = [&](int q) {
+            x = __fsub_rn(x, (float)sx[q]);
+            y = __fsub_rn(y, (float)sy[q]);
+            if (Z3) z = __fsub_rn(z, (float)sz[q]);
+        };
+        auto emit = [&]() {
+            const float fc = (float)cnt;
+            X[pi] = __fdiv_rn(x, fc);
+            Y[pi] = __fdiv_rn(y, fc);
+            if (Z3) Zo[pi] = __fdiv_rn(z, fc);
+            pi++;
+        };
+        for (int q = 1; q <= span; q++) {
+            add(2 * q - 1);
+            add(2 * q);
+            cnt += 2;
+            emit();
         }
+        for (int q = span + 1; q < n - span; q++) {
+            add(q + span);
+            sub(q - span - 1);
+            emit();
+        }
+        for (int q = n - span, d = span; q < n; q++, d--) {
+            sub(q - d - 1);
+            sub(q - d);
+            cnt -= 2;
+            emit();
+        }
+    }
+}
+
+static int prune_smooth_device(bgt_ctx *c, const DevSegs &s, int dims, int max_segment_length, int smoothing_span,
+                               float **ox, float **oy, float **oz, unsigned int **oidx, unsigned int *nsegs_out)
+{
+    cudaStream_t st = c->stream;
+    const int S = s.nseg;
+    unsigned nsegs = 0, npts = 0;
+    int *keep = nullptr, *kpts = nullptr, *seg_new = nullptr, *pt_new = nullptr;
+    cudaError_t e;
+    if (S > 0) {
+        void *p;
+        int rc = ctx_scratch(c, 21, (size_t)(S + 1) * 16, &p);
+        if (rc != BGT_OK) return rc;
+        keep = (int *)p;
+        kpts = keep + (S + 1);
+        seg_new = kpts + (S + 1);
+        pt_new = seg_new + (S + 1);
+        const int grid = std::min((S + 255) / 256, 148 * 8);
+        const unsigned long long maxlen = (unsigned long long)(long long)max_segment_length;
+        prune_flags_kernel<<<grid, 256, 0, st>>>(s.start, s.is_end, S, maxlen, keep, kpts);
+        cudaMemsetAsync(keep + S, 0, 4, st);
+        cudaMemsetAsync(kpts + S, 0, 4, st);
+        if ((e = exscan(c, 14, keep, seg_new, S + 1, st)) != cudaSuccess ||
+            (e = exscan(c, 14, kpts, pt_new, S + 1, st)) != cudaSuccess)
+            return cuda_fail(e, "prune scan");
+        int tot[2] = {0, 0};
+        if ((e = cudaMemcpyAsync(&tot[0], seg_new + S, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(&tot[1], pt_new + S, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return cuda_fail(e, "prune totals");
+        nsegs = (unsigned)tot[0];
+        npts = (unsigned)tot[1];
     }
     float *X = (float *)malloc(sizeof(float) * std::max(1u, npts));
     float *Y = (float *)malloc(sizeof(float) * std::max(1u, npts));
     float *Z = dims == 3 ? (float *)malloc(sizeof(float) * std::max(1u, npts)) : nullptr;
     unsigned *I = (unsigned *)malloc(sizeof(unsigned) * (nsegs + 1));
+    auto release = [&]() {
+        free(X);
+        free(Y);
+        free(Z);
+        free(I);
+    };
     if (!X || !Y || !I || (dims == 3 && !Z)) {
-        free(X); free(Y); free(Z); free(I);
+        release();
         return fail(BGT_ERR_NOMEM, "host allocation of centreline arrays");
     }
-    const int span_req = std::max(0, smoothing_span);
-    unsigned si = 0, pi = 0;
-    for (int k = 0; k < s.nseg; k++) {
-        const int b = s.start[k], n = s.start[k + 1] - s.start[k];
-        if (!((size_t)n > maxlen) && s.is_end[k]) continue;
-        I[si++] = pi;
-        const int16_t *px = s.px + b, *py = s.py + b, *pz = dims == 3 ? s.pz + b : nullptr;
-        const int span = std::min(span_req, (n - 1) / 2);
-        float x = px[0], y = py[0], z = pz ? pz[0] : 0.f;
-        int cnt = 1;
-        X[pi] = (float)px[0];
-        Y[pi] = (float)py[0];
-        if (Z) Z[pi] = (float)pz[0];
-        pi++;
-        auto emit = [&]() {
-            X[pi] = x / (float)cnt;
-            Y[pi] = y / (float)cnt;
-            if (Z) Z[pi] = z / (float)cnt;
-            pi++;
-        };
-        for (int q = 1; q <= span; q++) {
-            x += px[2 * q - 1]; y += py[2 * q - 1]; if (pz) z += pz[2 * q - 1];
-            x += px[2 * q];     y += py[2 * q];     if (pz) z += pz[2 * q];
-            cnt += 2;
-            emit();
+    if (nsegs > 0) {
+        const size_t fb = ((size_t)npts * 4 + 255) / 256 * 256;
+        void *p;
+        int rc = ctx_scratch(c, 22, 3 * fb + (size_t)(nsegs + 1) * 4, &p);
+        if (rc != BGT_OK) {
+            release();
+            return rc;
         }
-        for (int q = span + 1; q < n - span; q++) {
-            x += px[q + span]; y += py[q + span]; if (pz) z += pz[q + span];
-            x -= px[q - span - 1]; y -= py[q - span - 1]; if (pz) z -= pz[q - span - 1];
-            emit();
-        }
-        for (int q = n - span, d = span; q < n; q++, d--) {
-            x -= px[q - d - 1]; y -= py[q - d - 1]; if (pz) z -= pz[q - d - 1];
-            x -= px[q - d];     y -= py[q - d];     if (pz) z -= pz[q - d];
-            cnt -= 2;
-            emit();
+        float *dX = (float *)p, *dY = (float *)((char *)p + fb), *dZ = (float *)((char *)p + 2 * fb);
+        unsigned *dI = (unsigned *)((char *)p + 3 * fb);
+        const int grid = std::min((S + 127) / 128, 148 * 8);
+        const int span = std::max(0, smoothing_span);
+        if (dims == 3)
+            smooth_kernel<true><<<grid, 128, 0, st>>>(s.start, s.px, s.py, s.pz, keep, seg_new, pt_new, S, span, dX,
+                                                       dY, dZ, dI);
+        else
+            smooth_kernel<false><<<grid, 128, 0, st>>>(s.start, s.px, s.py, nullptr, keep, seg_new, pt_new, S, span,
+                                                        dX, dY, nullptr, dI);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(X, dX, (size_t)npts * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(Y, dY, (size_t)npts * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && dims == 3) e = cudaMemcpyAsync(Z, dZ, (size_t)npts * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(I, dI, (size_t)nsegs * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            release();
+            return cuda_fail(e, "centreline readback");
         }
     }
     I[nsegs] = npts;
@@ -181,7 +272,7 @@ static int prune_smooth(const HostSegs &s, int dims, int max_segment_length, int
 }
 
 // Thin the padded image with the engine and extract segments on the device.
-static int centerline_segments(bgt_ctx *c, int dims, int dtype, const void *in, int w, int h, int d, HostSegs *hs)
+static int centerline_segments(bgt_ctx *c, int dims, int dtype, const void *in, int w, int h, int d, DevSegs *ds)
 {
     if (!c || !in) return fail(BGT_ERR_ARG, "null argument");
     const size_t es = dtype_size(dtype);
@@ -213,7 +304,7 @@ static int centerline_segments(bgt_ctx *c, int dims, int dtype, const void *in, 
     if (rc == BGT_OK) rc = batch_check(b);
     if (rc != BGT_OK) return rc;
     const Inst &inst = b->h[0];
-    return segments_packed(c, dims, inst.buf[0], pw, ph, pd, inst.P, hs);
+    return segments_device_arrays(c, dims, inst.buf[0], pw, ph, pd, inst.P, ds);
 }
 
 extern "C" int bgt_centerline2d(bgt_ctx *c, int dtype, const void *in, int w, int h, int max_segment_length,
@@ -221,11 +312,10 @@ extern "C" int bgt_centerline2d(bgt_ctx *c, int dtype, const void *in, int w, in
                                 unsigned int *nsegs)
 {
     if (!out_x || !out_y || !out_idx || !nsegs) return fail(BGT_ERR_ARG, "null output");
-    HostSegs hs;
-    int rc = centerline_segments(c, 2, dtype, in, w, h, 1, &hs);
+    DevSegs ds;
+    int rc = centerline_segments(c, 2, dtype, in, w, h, 1, &ds);
     if (rc == BGT_OK)
-        rc = prune_smooth(hs, 2, max_segment_length, smoothing_span, out_x, out_y, nullptr, out_idx, nsegs);
-    free_host_segs(&hs);
+        rc = prune_smooth_device(c, ds, 2, max_segment_length, smoothing_span, out_x, out_y, nullptr, out_idx, nsegs);
     return rc;
 }
 
@@ -234,10 +324,9 @@ extern "C" int bgt_centerline3d(bgt_ctx *c, int dtype, const void *in, int w, in
                                 unsigned int **out_idx, unsigned int *nsegs)
 {
     if (!out_x || !out_y || !out_z || !out_idx || !nsegs) return fail(BGT_ERR_ARG, "null output");
-    HostSegs hs;
-    int rc = centerline_segments(c, 3, dtype, in, w, h, d, &hs);
+    DevSegs ds;
+    int rc = centerline_segments(c, 3, dtype, in, w, h, d, &ds);
     if (rc == BGT_OK)
-        rc = prune_smooth(hs, 3, max_segment_length, smoothing_span, out_x, out_y, out_z, out_idx, nsegs);
-    free_host_segs(&hs);
+        rc = prune_smooth_device(c, ds, 3, max_segment_length, smoothing_span, out_x, out_y, out_z, out_idx, nsegs);
     return rc;
 }

@@ -55,8 +55,20 @@ struct HostSegs {
     uint8_t *is_end = nullptr;
     int16_t *px = nullptr, *py = nullptr, *pz = nullptr;
 };
-// Device ExtractSegmentsV on a packed image (P words per row).
+// Segment arrays in device memory (same layout as HostSegs; null when empty).
+struct DevSegs {
+    int nseg = 0, npts = 0;
+    int32_t *start = nullptr;
+    uint8_t *is_end = nullptr;
+    int16_t *px = nullptr, *py = nullptr, *pz = nullptr;
+};
+// Device ExtractSegmentsV on a packed image (P words per row): arrays left in
+// the context's scratch, or copied to host memory.
+int segments_device_arrays(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, int D, int P, DevSegs *out);
 int segments_packed(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, int D, int P, HostSegs *out);
+// Exclusive prefix sum of n ints on the context's stream (CUB temporary
+// storage in scratch slot `slot`).
+cudaError_t exscan(bgt_ctx *c, int slot, const int *in, int *out, long long n, cudaStream_t st);
 void free_host_segs(HostSegs *s);
 }  // namespace bgt
 

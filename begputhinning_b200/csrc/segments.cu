@@ -324,7 +324,7 @@ static int grid_of(long long n, int block = 256)
 }
 
 // Exclusive sum via CUB; temp storage from scratch slot `slot`.
-static cudaError_t exscan(bgt_ctx *c, int slot, const int *in, int *out, long long n, cudaStream_t st)
+cudaError_t exscan(bgt_ctx *c, int slot, const int *in, int *out, long long n, cudaStream_t st)
 {
     size_t tb = 0;
     cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, (int)n, st);
@@ -335,8 +335,9 @@ static cudaError_t exscan(bgt_ctx *c, int slot, const int *in, int *out, long lo
 }
 
 // Device segment extraction on a packed image (P words per row, H rows, D
-// planes; W x H x D pixels).  Fills host arrays.
-int segments_packed(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, int D, int P, HostSegs *out)
+// planes; W x H x D pixels).  The segment arrays stay in the context's
+// scratch (slot 19) until the next extraction on the context.
+int segments_device_arrays(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, int D, int P, DevSegs *out)
 {
     cudaStream_t st = c->stream;
     const long long npx = (long long)W * H * D;
@@ -366,16 +367,8 @@ int segments_packed(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, i
     if ((e = cudaMemcpyAsync(&nn, offs + nw, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return cuda_fail(e, "node count");
-    *out = HostSegs();
-    if (nn == 0) {
-        out->start = (int32_t *)malloc(4);
-        out->start[0] = 0;
-        out->is_end = (uint8_t *)malloc(1);
-        out->px = (int16_t *)malloc(2);
-        out->py = (int16_t *)malloc(2);
-        if (dims == 3) out->pz = (int16_t *)malloc(2);
-        return BGT_OK;
-    }
+    *out = DevSegs();
+    if (nn == 0) return BGT_OK;
     void *p5, *p7, *p8, *p9, *p10, *p11, *p12, *p13, *p15, *p16, *p17, *p18;
     if ((rc = ctx_scratch(c, 5, (size_t)nn * 4, &p5)) || (rc = ctx_scratch(c, 7, (size_t)nn * 4, &p7)) ||
         (rc = ctx_scratch(c, 8, (size_t)nn * 4, &p8)) || (rc = ctx_scratch(c, 9, (size_t)nn * 4, &p9)) ||
@@ -462,6 +455,25 @@ int segments_packed(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, i
     cudaMemcpyAsync(wo.start + S, pt_off + nn, 4, cudaMemcpyDeviceToDevice, st);
     out->nseg = S;
     out->npts = Np;
+    out->start = wo.start;
+    out->is_end = wo.is_end;
+    out->px = wo.px;
+    out->py = wo.py;
+    out->pz = dims == 3 ? wo.pz : nullptr;
+    return BGT_OK;
+}
+
+// The same, with the segment arrays copied to host memory (malloc).
+int segments_packed(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, int D, int P, HostSegs *out)
+{
+    DevSegs ds;
+    int rc = segments_device_arrays(c, dims, d_buf, W, H, D, P, &ds);
+    if (rc != BGT_OK) return rc;
+    cudaStream_t st = c->stream;
+    const int S = ds.nseg, Np = ds.npts;
+    *out = HostSegs();
+    out->nseg = S;
+    out->npts = Np;
     out->start = (int32_t *)malloc((size_t)(S + 1) * 4);
     out->is_end = (uint8_t *)malloc((size_t)S + 1);
     out->px = (int16_t *)malloc((size_t)Np * 2 + 2);
@@ -469,12 +481,16 @@ int segments_packed(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, int H, i
     out->pz = dims == 3 ? (int16_t *)malloc((size_t)Np * 2 + 2) : nullptr;
     if (!out->start || !out->is_end || !out->px || !out->py || (dims == 3 && !out->pz))
         return fail(BGT_ERR_NOMEM, "host allocation of segment arrays");
-    e = cudaMemcpyAsync(out->start, wo.start, (size_t)(S + 1) * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out->is_end, wo.is_end, (size_t)S, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out->px, wo.px, (size_t)Np * 2, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out->py, wo.py, (size_t)Np * 2, cudaMemcpyDeviceToHost, st);
+    if (S == 0) {
+        out->start[0] = 0;
+        return BGT_OK;
+    }
+    cudaError_t e = cudaMemcpyAsync(out->start, ds.start, (size_t)(S + 1) * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out->is_end, ds.is_end, (size_t)S, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out->px, ds.px, (size_t)Np * 2, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out->py, ds.py, (size_t)Np * 2, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && dims == 3)
-        e = cudaMemcpyAsync(out->pz, wo.pz, (size_t)Np * 2, cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(out->pz, ds.pz, (size_t)Np * 2, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(e, "segment readback");
     return BGT_OK;

@@ -55,6 +55,7 @@ struct Slot {
     cudaEvent_t done = nullptr;
     bool busy = false;      // holds admitted requests
     bool launched = false;  // its work (ending with `done`) is enqueued
+    int cfg = -1;           // tile configuration of the lane (-1: tuned / default)
     std::vector<Req *> reqs;
 };
 
@@ -111,7 +112,8 @@ int launch_slot(bgt_server *S, Slot &s)
     if (e != cudaSuccess) return cuda_fail(e, "serve H2D");
     for (size_t i = 0; i < s.reqs.size() && rc == BGT_OK; i++) {
         const Req *r = s.reqs[i];
-        rc = r->dims == 2 ? bgt_batch_add2d(b, r->w, r->h, -1, nullptr) : bgt_batch_add3d(b, r->w, r->h, r->d, -1, nullptr);
+        rc = r->dims == 2 ? bgt_batch_add2d(b, r->w, r->h, s.cfg, nullptr)
+                          : bgt_batch_add3d(b, r->w, r->h, r->d, s.cfg, nullptr);
     }
     if (rc == BGT_OK) rc = bgt_batch_finalize(b);
     for (size_t i = 0; i < s.reqs.size() && rc == BGT_OK; i++)
@@ -222,7 +224,7 @@ void completer_loop(bgt_server *S)
 }
 
 int setup_lane(bgt_server *S, int li, int dims, int priority, int nslots, int max_batch, size_t io_cap,
-               size_t pool_bytes, int grid_cap)
+               size_t pool_bytes, int grid_cap, int cfg)
 {
     Lane &L = S->lane[li];
     L.dims = dims;
@@ -230,6 +232,7 @@ int setup_lane(bgt_server *S, int li, int dims, int priority, int nslots, int ma
     L.pool_bytes = pool_bytes;
     L.slots.resize(nslots);
     for (Slot &s : L.slots) {
+        s.cfg = cfg;
         if (S->reserved + io_cap + pool_bytes > S->budget)
             return fail(BGT_ERR_LIMIT, "serving slots exceed the HBM budget (%zu bytes)", S->budget);
         int rc = bgt_ctx_create(S->device, &s.ctx);
@@ -290,10 +293,12 @@ extern "C" int bgt_server_create(int device, size_t hbm_budget_bytes, bgt_server
     const size_t MiB = size_t(1) << 20;
     // frames: 16 x (1024^2 in + out) per slot, packed pools are small; two
     // slots with one CTA per SM each
-    int rc = setup_lane(S, 0, 2, hi, 2, 16, 16 * 2 * MiB + 8 * MiB, 64 * MiB, sms);
+    int rc = setup_lane(S, 0, 2, hi, 2, 16, 16 * 2 * MiB + 8 * MiB, 64 * MiB, sms, -1);
     // volumes: 4 x 320^3 in + out per slot; three slots with one CTA per SM
-    // each, so frames always find room on every SM
-    if (rc == BGT_OK) rc = setup_lane(S, 1, 3, lo, 3, 4, 4 * 2 * 33 * MiB, 192 * MiB, sms);
+    // each, so frames always find room on every SM.  Volumes use 16-plane
+    // tiles: the least total work per pass (fewest halo planes), which is
+    // what a throughput lane sharing the GPU with latency-bound frames wants
+    if (rc == BGT_OK) rc = setup_lane(S, 1, 3, lo, 3, 4, 4 * 2 * 33 * MiB, 192 * MiB, sms, 17);
     if (rc != BGT_OK) {
         teardown(S);
         delete S;
