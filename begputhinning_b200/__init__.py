@@ -5,7 +5,8 @@ BEGPUThinning.  The compute path is libbgt.so (hand-written sm_100a CUDA
 behind a C ABI, include/bgt_capi.h); this package is the Python host side."""
 from ._lib import BGTError, lib
 from .api import (Batch, CenterlineExtraction, Context, ExtractSegmentsV, PipelinedBatch, Segments, Thinning2D,
-                  Thinning3D, cfg_describe, cfg_list, default_context, thin_device)
+                  Thinning3D, cfg_describe, cfg_list, default_context, matlab_segments, thin_device)
 
-__all__ = ["BGTError", "lib", "Batch", "CenterlineExtraction", "Context", "ExtractSegmentsV", "PipelinedBatch", "Segments",
-           "Thinning2D", "Thinning3D", "cfg_describe", "cfg_list", "default_context", "thin_device"]
+__all__ = ["BGTError", "lib", "Batch", "CenterlineExtraction", "Context", "ExtractSegmentsV", "PipelinedBatch",
+           "Segments", "Thinning2D", "Thinning3D", "cfg_describe", "cfg_list", "default_context", "matlab_segments",
+           "thin_device"]

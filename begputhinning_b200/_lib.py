@@ -14,7 +14,7 @@ SYNTH_PATH = os.path.join(PKG, "libbgt_synth.so")
 EXPORTS = [
     "bgt_ctx_create", "bgt_ctx_destroy", "bgt_ctx_set_stream", "bgt_last_error", "bgt_version",
     "bgt_thin2d", "bgt_thin3d", "bgt_thin2d_device", "bgt_thin3d_device", "bgt_thin2d_device_noalloc",
-    "bgt_centerline2d", "bgt_centerline3d", "bgt_free",
+    "bgt_centerline2d", "bgt_centerline3d", "bgt_free", "bgt_matlab_segments",
     "bgt_segments2d_device", "bgt_segments3d_device",
     "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
     "bgt_batch_reserve", "bgt_batch_reset", "bgt_batch_set_grid",
@@ -82,6 +82,7 @@ def _declare(L):
         "bgt_tune_get": [I, I, ip],
         "bgt_cfg_list": [I, ip, I, ip],
         "bgt_cfg_describe": [I, ip, ip, ip, ip, ip, ip],
+        "bgt_matlab_segments": [I, C.c_uint, vp, vp, vp, vp, vp],
         "bgt_rule_table": [I, I, vp, vp],
         "bgt_server_create": [I, C.c_size_t, C.POINTER(vp)],
         "bgt_server_submit": [vp, I, vp, I, I, I, vp, C.POINTER(C.c_ulonglong)],

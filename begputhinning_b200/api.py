@@ -171,6 +171,28 @@ def CenterlineExtraction(data: np.ndarray, max_segment_length: int, smoothing_sp
     return x, y, idx
 
 
+def matlab_segments(x: np.ndarray, y: np.ndarray, idx: np.ndarray, z: np.ndarray | None = None) -> list:
+    """Centreline output in the MATLAB gateways' cell layout: one
+    (ssize, 2) array per segment with columns y, x — (ssize, 3) with y, x, z
+    in 3-D — in column-major (Fortran) order, doubles; formatted by
+    bgt_matlab_segments."""
+    dims = 2 if z is None else 3
+    idx = np.ascontiguousarray(idx, np.uint32)
+    nsegs = len(idx) - 1
+    npts = int(idx[-1]) if nsegs >= 0 else 0
+    xs = np.ascontiguousarray(x, np.float32)
+    ys = np.ascontiguousarray(y, np.float32)
+    zs = None if z is None else np.ascontiguousarray(z, np.float32)
+    out = np.empty(max(1, dims * npts), np.float64)
+    check(lib().bgt_matlab_segments(dims, nsegs, _vp(xs), _vp(ys), None if zs is None else _vp(zs), _vp(idx),
+                                    _vp(out)))
+    cells = []
+    for i in range(nsegs):
+        b, n = dims * int(idx[i]), int(idx[i + 1] - idx[i])
+        cells.append(out[b:b + dims * n].reshape(n, dims, order="F"))
+    return cells
+
+
 @dataclass
 class Segments:
     """ExtractSegmentsV output in emission order."""

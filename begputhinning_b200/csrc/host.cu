@@ -856,3 +856,22 @@ extern "C" int bgt_thin3d(bgt_ctx *c, int dtype, const void *in, int w, int h, i
 }
 
 extern "C" void bgt_free(void *p) { free(p); }
+
+extern "C" int bgt_matlab_segments(int dims, unsigned int nsegs, const float *x, const float *y, const float *z,
+                                   const unsigned int *idx, double *out)
+{
+    if (dims != 2 && dims != 3) return fail(BGT_ERR_ARG, "dims must be 2 or 3");
+    if (!idx || (nsegs > 0 && (!x || !y || !out || (dims == 3 && !z)))) return fail(BGT_ERR_ARG, "null argument");
+    for (unsigned i = 0; i < nsegs; i++) {
+        if (idx[i + 1] < idx[i]) return fail(BGT_ERR_ARG, "idx is not ascending at segment %u", i);
+        const size_t n = idx[i + 1] - idx[i];
+        double *m = out + (size_t)dims * idx[i];
+        for (size_t t = 0; t < n; t++) {
+            const size_t p = idx[i] + t;
+            m[t] = (double)y[p];
+            m[n + t] = (double)x[p];
+            if (dims == 3) m[2 * n + t] = (double)z[p];
+        }
+    }
+    return BGT_OK;
+}

@@ -106,6 +106,16 @@ int bgt_centerline3d(bgt_ctx *ctx, int dtype, const void *in, int width, int hei
                      unsigned int **out_idx, unsigned int *nsegs);
 void bgt_free(void *p);
 
+/* MATLAB column order of centreline output, as the reference's MEX gateways
+ * build their cell arrays (2D/Matlab2DThinning.cpp:163-175,
+ * 3D/Matlab3DThinning.cpp:157-171): segment i becomes an ssize x dims
+ * column-major double matrix whose columns are y, x (and z), ssize =
+ * idx[i+1] - idx[i].  The matrices are written back to back into out
+ * (dims * idx[nsegs] doubles; segment i starts at out + dims * idx[i]).
+ * z is ignored (may be null) when dims == 2.  Host memory, no device work. */
+int bgt_matlab_segments(int dims, unsigned int nsegs, const float *x, const float *y, const float *z,
+                        const unsigned int *idx, double *out);
+
 /* ---- segment extraction on the device -------------------------------
  * Replace ExtractSegmentsV<T> (2D/ExtractSegments.h:16-17,
  * 3D/ExtractSegments.h:21-22) on a thinned 0/1 image already in device
