@@ -50,7 +50,7 @@ struct alignas(16) Inst {
     uint32_t *uni;            // 3D pre-test union (per word), null in 2D
     const CUtensorMap *tmap;  // [3] tensor maps over buf[0], buf[1], uni (3D)
     int *lc;                  // per-tile pass of the last change (kNever: empty tile)
-    uint8_t *act;             // per-tile activity of the current iteration (3D)
+    uint8_t *act;             // 3D: activity of the current iteration; 2D: border bands of the last change
     int *list;                // active tile ids of the wave in flight
     // engine state (device-side scheduler)
     int pass;                 // pass of the wave in flight

@@ -102,24 +102,25 @@ __device__ void issue_tile(const Inst &in, int q, int tile, uint32_t *smem, uint
 }
 
 // Run one tile of instance `in` at pass q with the instance's configuration
-// on its box, already in smem.  All tile threads call it.
-__device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem)
+// on its box, already in smem.  All tile threads call it; returns the change
+// mask (complete in thread 0; `band` is a zeroed shared word it may use).
+__device__ uint32_t run_tile(const Inst &in, int q, int tile, uint32_t *smem, uint32_t *band)
 {
     switch (in.cfg) {
 #define CASE2_K1(ID, C)                                    \
     case ID:                                               \
         switch (q & 3) {                                   \
-        case 0: return tile2d<C, 0>(in, q, tile, smem);   \
-        case 1: return tile2d<C, 1>(in, q, tile, smem);   \
-        case 2: return tile2d<C, 2>(in, q, tile, smem);   \
-        default: return tile2d<C, 3>(in, q, tile, smem);  \
+        case 0: return tile2d<C, 0>(in, q, tile, smem, band);   \
+        case 1: return tile2d<C, 1>(in, q, tile, smem, band);   \
+        case 2: return tile2d<C, 2>(in, q, tile, smem, band);   \
+        default: return tile2d<C, 3>(in, q, tile, smem, band);  \
         }
 #define CASE2_K2(ID, C)                                         \
     case ID:                                                    \
-        if (q & 1) return tile2d<C, 2>(in, q, tile, smem);     \
-        return tile2d<C, 0>(in, q, tile, smem);
+        if (q & 1) return tile2d<C, 2>(in, q, tile, smem, band);     \
+        return tile2d<C, 0>(in, q, tile, smem, band);
 #define CASE2_K4(ID, C) \
-    case ID: return tile2d<C, 0>(in, q, tile, smem);
+    case ID: return tile2d<C, 0>(in, q, tile, smem, band);
 #define CASE2X(ID, C) \
     case ID: return tile2dx<C, 0>(in, q, tile, smem);
 #define CASE3(ID, C)                                       \
@@ -154,7 +155,7 @@ __device__ bool run_tile(const Inst &in, int q, int tile, uint32_t *smem)
 #undef CASE2X
 #undef CASE3
     default:
-        return false;
+        return 0u;
     }
 }
 
@@ -664,9 +665,11 @@ __global__ void __launch_bounds__(kThreads) plain_pass_kernel(Inst *pin, int q, 
     uint32_t *smem = align128(smem_raw);
     __shared__ __align__(8) uint64_t bar;
     __shared__ int active;
+    __shared__ uint32_t band;
     const Inst &in = *pin;
     const int tile = blockIdx.x;
     if (threadIdx.x == 0) {
+        band = 0;
         bool a;
         if (in.dims == 3 && q % 6 != 0) {
             a = in.act[tile] != 0;
@@ -686,7 +689,7 @@ __global__ void __launch_bounds__(kThreads) plain_pass_kernel(Inst *pin, int q, 
     if (!mbar_wait_bounded(&bar, 0)) {
         if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
     }
-    const bool ch = run_tile(in, q, tile, smem);
+    const bool ch = (run_tile(in, q, tile, smem, &band) & kTileChanged) != 0;
     if (threadIdx.x == 0) {
         atomicAdd(&pin->tiles_run, 1ull);
         atomicAdd(&pin->work_words, (unsigned long long)tile_core_words(in, tile));
@@ -785,11 +788,15 @@ __device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int s
         for (int i = threadIdx.x; i < 2 * nwords; i += kTileThreads) scratch[i] = 0;
         tile_sync();
         const int tx = in.tiles_x, ty = in.tiles_y, tz = in.tiles_z;
+        // 2D tiles fused over a whole iteration (window 1) recorded which
+        // neighbours their change reaches (border bands); others reach all
+        const bool bands = in.dims == 2 && window == 1;
         for (int t = threadIdx.x; t < nt; t += kTileThreads) {
             const int v = ld_cg_int(in.lc + t);
             if (v == kNever) continue;
             atomicOr(ne + (t >> 5), 1u << (t & 31));
             if (v < thr) continue;
+            const uint32_t reach = (bands && v >= 0) ? (uint32_t)__ldcg(in.act + t) : kAllBands;
             const int x = t % tx, y = (t / tx) % ty, z = t / (tx * ty);
             for (int dz = -1; dz <= 1; dz++) {
                 const int zz = z + dz;
@@ -800,6 +807,7 @@ __device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int s
                     for (int dx = -1; dx <= 1; dx++) {
                         const int xx = x + dx;
                         if (xx < 0 || xx >= tx) continue;
+                        if ((dy | dx) != 0 && dz == 0 && !((reach >> band_bit(dy, dx)) & 1u)) continue;
                         const int u = (zz * ty + yy) * tx + xx;
                         atomicOr(act + (u >> 5), 1u << (u & 31));
                     }
@@ -924,7 +932,9 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
     __shared__ __align__(8) uint64_t bar;
     __shared__ int4 item;
     __shared__ int got, last;
+    __shared__ uint32_t band;
     if (threadIdx.x == 0) {
+        band = 0;
         mbar_init(&bar, 1);
         fence_mbar_init();
     }
@@ -969,9 +979,12 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
             if (threadIdx.x == 0) atomicOr(&S->status, kErrTmaTimeout);
         }
         parity ^= 1u;
-        const bool ch = run_tile(in, q, tile, smem);  // ends with a barrier: smem is free again
+        const uint32_t m = run_tile(in, q, tile, smem, &band);  // ends with a barrier: smem is free again
         if (threadIdx.x == 0) {
-            if (ch) in.lc[tile] = q;
+            if (m & kTileChanged) {
+                in.lc[tile] = q;
+                if (in.dims == 2) in.act[tile] = (uint8_t)(m & kAllBands);  // bands the next wave reads
+            }
             __threadfence();
             const int d = atomicAdd(&in.done, 1);
             last = d == nwave - 1;

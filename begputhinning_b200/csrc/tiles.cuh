@@ -27,6 +27,18 @@
 
 namespace bgt {
 
+// ------------------------------------------------------------ changes -----
+// A tile reports its change as a mask: kTileChanged when any core pixel was
+// deleted, plus one bit per neighbour tile whose K-pixel ring reaches a
+// deleted pixel (bit band_bit(dy, dx) for the neighbour at offset (dy, dx)).
+// Tiles that do not work out the bands report all of them.
+constexpr uint32_t kTileChanged = 0x100u;
+constexpr uint32_t kAllBands = 0xFFu;
+__host__ __device__ constexpr int band_bit(int dy, int dx)
+{
+    return (dy + 1) * 3 + (dx + 1) - ((dy + 1) * 3 + (dx + 1) > 4 ? 1 : 0);
+}
+
 // ---------------------------------------------------------------- 2D ------
 // One subiteration on the lane's S+2 words.  Word steps whose centre words
 // are empty in every lane of the warp are skipped (nothing to delete there).
@@ -90,10 +102,11 @@ __device__ __forceinline__ void tile2d_issue(const Inst &in, int q, int tile, ui
 }
 
 // Process one 2D tile for pass q (phase PH = first direction of the pass)
-// from its box in smem.  Returns (to all tile threads) whether any core
-// pixel was deleted.
+// from its box in smem.  Returns the change mask: to thread 0 with the
+// border bands (accumulated in *band, which it resets), to the other tile
+// threads kTileChanged or 0.
 template <class C, int PH>
-__device__ bool tile2d(const Inst &in, int q, int tile, const uint32_t *smem)
+__device__ uint32_t tile2d(const Inst &in, int q, int tile, const uint32_t *smem, uint32_t *band)
 {
     constexpr int K = C::kK, S = C::kS, CORE = C::CORE, BW = C::BW;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -124,6 +137,7 @@ __device__ bool tile2d(const Inst &in, int q, int tile, const uint32_t *smem)
     for (int c = 0; c < S; c++) chg |= v[1 + c] ^ row[4 + c];
     const int y = y0 + r - K;  // image row of this lane
     const bool core = lane >= K && lane < 32 - K && y < in.H;
+    uint32_t bm = 0;
     if (core) {
         uint32_t *drow = dst + (size_t)y * in.P + x0;
 #pragma unroll
@@ -131,8 +145,26 @@ __device__ bool tile2d(const Inst &in, int q, int tile, const uint32_t *smem)
             if (x0 + 4 * c < in.P)
                 *reinterpret_cast<uint4 *>(drow + 4 * c) =
                     make_uint4(v[1 + 4 * c], v[2 + 4 * c], v[3 + 4 * c], v[4 + 4 * c]);
+        // border bands: the first/last K core rows and the K pixels at each
+        // x edge reach into the ring of the neighbour on that side
+        const int cr = r - K;  // core row within the tile
+        const bool top = cr < K, bot = cr >= C::TH - K;
+        const bool lft = ((v[1] ^ row[4]) & ((1u << K) - 1u)) != 0;
+        const bool rgt = ((v[S] ^ row[S + 3]) & ~(0xFFFFFFFFu >> K)) != 0;
+        const bool any = chg != 0;
+        bm = (top && any ? 1u << band_bit(-1, 0) : 0u) | (bot && any ? 1u << band_bit(1, 0) : 0u) |
+             (lft ? 1u << band_bit(0, -1) : 0u) | (rgt ? 1u << band_bit(0, 1) : 0u) |
+             (top && lft ? 1u << band_bit(-1, -1) : 0u) | (top && rgt ? 1u << band_bit(-1, 1) : 0u) |
+             (bot && lft ? 1u << band_bit(1, -1) : 0u) | (bot && rgt ? 1u << band_bit(1, 1) : 0u);
     }
-    return tile_sync_or(core && chg != 0);
+    bm = __reduce_or_sync(kFull, bm);
+    if (lane == 0 && bm) atomicOr(band, bm);
+    uint32_t m = tile_sync_or(core && chg != 0) ? kTileChanged : 0u;
+    if (threadIdx.x == 0) {
+        m |= *band;
+        *band = 0;
+    }
+    return m;
 }
 
 // ------------------------------------------- 2D, shared warp edges -------
@@ -223,7 +255,7 @@ __device__ __forceinline__ void run_subits2d_x(uint32_t (&v)[C::kS + 2], uint32_
 }
 
 template <class C, int PH>
-__device__ bool tile2dx(const Inst &in, int q, int tile, uint32_t *smem)
+__device__ uint32_t tile2dx(const Inst &in, int q, int tile, uint32_t *smem)
 {
     constexpr int K = C::kK, S = C::kS, BW = C::BW, BH = C::BH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -259,7 +291,7 @@ __device__ bool tile2dx(const Inst &in, int q, int tile, uint32_t *smem)
                 *reinterpret_cast<uint4 *>(drow + 4 * c) =
                     make_uint4(v[1 + 4 * c], v[2 + 4 * c], v[3 + 4 * c], v[4 + 4 * c]);
     }
-    return tile_sync_or(core && chg != 0);
+    return tile_sync_or(core && chg != 0) ? kTileChanged | kAllBands : 0u;
 }
 
 // ---------------------------------------------------------------- 3D ------
@@ -314,7 +346,7 @@ __device__ __forceinline__ void tile3d_issue(const Inst &in, int q, int tile, ui
 
 // MODE 0: pre-test union (stored) + U.  MODE 1..5: N, E, D, S, W.
 template <class C, int MODE>
-__device__ bool tile3d(const Inst &in, int q, int tile, const uint32_t *smem)
+__device__ uint32_t tile3d(const Inst &in, int q, int tile, const uint32_t *smem)
 {
     constexpr int NWX = C::kNWX, TZ = C::kTZ, BW = C::BW, BH = C::BH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -374,7 +406,7 @@ __device__ bool tile3d(const Inst &in, int q, int tile, const uint32_t *smem)
     }
     // the barrier orders every thread's stores before thread 0's fence and
     // release (engine) or the end of the launch (plain path)
-    return tile_sync_or(chg != 0u);
+    return tile_sync_or(chg != 0u) ? kTileChanged | kAllBands : 0u;
 }
 
 // ------------------------------------------------------------ activity ----
