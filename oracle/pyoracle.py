@@ -320,6 +320,8 @@ def ref_gpu_thin2d(img: np.ndarray) -> np.ndarray:
     h, w = a.shape
     if w > 1024:
         raise ValueError("the reference 2D kernel is out of bounds for widths above 1024")
+    if h <= 64:
+        raise ValueError("the reference 2D launcher sizes an empty grid for heights up to 64")
     out = np.zeros_like(a)
     ref("2d_gpu").ref2d_gpu_thin_u8(w, h, _u8(a), _u8(out))
     return out
