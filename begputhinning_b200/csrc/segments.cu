@@ -205,18 +205,31 @@ __global__ void comp_starts_kernel(const int *__restrict__ flag, const int *__re
 
 // ------------------------------------------------------------- walk -------
 struct WalkOut {
-    // count pass
     int *nseg;   // [nn] per node (indexed by position in the raster-ordered list)
     int *npts;   // [nn]
-    // emit pass
-    const int *seg_off;  // [nn] exclusive scan of nseg
-    const int *pt_off;   // [nn] exclusive scan of npts
-    int32_t *start;      // [nseg_total + 1]
-    uint8_t *is_end;     // [nseg_total]
-    int16_t *px, *py, *pz;
+    int *tpo;    // [nn] the node's first point in the temporary arrays
+    int *tso;    // [nn] the node's first segment in the temporary arrays
+    const int *cpb;  // [ncomp+1] each component's first point in the temporary arrays
+    const int *csb;  // [ncomp+1] each component's first segment
+    int16_t *tx, *ty, *tz;  // temporary points in emission order, per component
+    int32_t *trel;          // temporary segment starts (point index within the node's output)
+    uint8_t *tend;          // temporary is_end flags
+    int *err;               // kErrSegOverflow when a component outgrows its bound
 };
 
-template <int DIMS, bool EMIT>
+// One warp per component replays the reference's walk over the component's
+// nodes in raster order (lanes read the 8/26 neighbours, a ballot picks the
+// first nonzero one in the reference's scan order).  Writes to the value map
+// are kept to the pixels that anything can look at again: a walk along a
+// chain zeroes its first and last chain pixels and every original node it
+// passes; the chain pixels in between (nn == 2, both neighbours on the same
+// walk) are skipped, because only a walk standing next to them could read
+// them and the chain is never entered again (its ends are zero).  The walk
+// excludes the pixel it came from, which the reference has zeroed.  A stall
+// (no nonzero neighbour) zeroes the pixel before it, so that the stalled
+// pixel's later walks see it as the reference does.  Coordinates follow the
+// steps instead of being divided out of the raster index.
+template <int DIMS>
 __global__ void walk_kernel(int8_t *V, const int8_t *__restrict__ V0, int W, int H,
                             const uint32_t *__restrict__ sorted_nodes, const uint32_t *__restrict__ sorted_rank,
                             const int *__restrict__ comp_start, int ncomp, int nn, WalkOut out)
@@ -225,8 +238,10 @@ __global__ void walk_kernel(int8_t *V, const int8_t *__restrict__ V0, int W, int
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const long long slice = (long long)W * H;
-    // this lane's neighbour offset in the reference's scan order
+    // this lane's neighbour offset in the reference's scan order, and its
+    // (dx, dy, dz) packed as (dz+1)*9 + (dy+1)*3 + (dx+1)
     long long my_off = 0;
+    int my_d = 13;
     {
         int q = 0;
         const int zlo = DIMS == 3 ? -1 : 0, zhi = DIMS == 3 ? 1 : 0;
@@ -234,7 +249,10 @@ __global__ void walk_kernel(int8_t *V, const int8_t *__restrict__ V0, int W, int
             for (int dy = -1; dy <= 1; dy++)
                 for (int dx = -1; dx <= 1; dx++) {
                     if (!dz && !dy && !dx) continue;
-                    if (q == lane) my_off = dz * slice + (long long)dy * W + dx;
+                    if (q == lane) {
+                        my_off = dz * slice + (long long)dy * W + dx;
+                        my_d = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+                    }
                     q++;
                 }
     }
@@ -242,13 +260,20 @@ __global__ void walk_kernel(int8_t *V, const int8_t *__restrict__ V0, int W, int
     for (int comp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; comp < ncomp; comp += warps) {
         const int a = comp_start[comp];
         const int b = comp + 1 < ncomp ? comp_start[comp + 1] : nn;
+        // the component's outputs go to its own temporary range, in emission order
+        int po = out.cpb[comp], so = out.csb[comp];
+        const int po_end = out.cpb[comp + 1], so_end = out.csb[comp + 1];
         for (int k = a; k < b; k++) {
             const long long p = sorted_nodes[k];
             const int rank = (int)sorted_rank[k];  // position in raster-ordered node list
             const int vp = V[p];
             __syncwarp();
+            if (lane == 0) {
+                out.tpo[rank] = po;
+                out.tso[rank] = so;
+            }
             if (vp >= 0) {
-                if (!EMIT && lane == 0) {
+                if (lane == 0) {
                     out.nseg[rank] = 0;
                     out.npts[rank] = 0;
                 }
@@ -256,50 +281,152 @@ __global__ void walk_kernel(int8_t *V, const int8_t *__restrict__ V0, int W, int
             }
             if (lane == 0) V[p] = 0;
             __syncwarp();
+            const int p_x = (int)(p % W), p_y = (int)((p / W) % H), p_z = DIMS == 3 ? (int)(p / slice) : 0;
             int ni = -1;
             int segs = 0, pts = 0;
-            int so = EMIT ? out.seg_off[rank] : 0, po = EMIT ? out.pt_off[rank] : 0;
-            auto put = [&](long long t) {
-                if (EMIT && lane == 0) {
-                    out.px[po] = (int16_t)(t % W);
-                    out.py[po] = (int16_t)((t / W) % H);
-                    if (DIMS == 3) out.pz[po] = (int16_t)(t / slice);
+            int cx = p_x, cy = p_y, cz = p_z;
+            auto put = [&]() {
+                if (lane == 0) {
+                    if (po < po_end) {
+                        out.tx[po] = (int16_t)cx;
+                        out.ty[po] = (int16_t)cy;
+                        if (DIMS == 3) out.tz[po] = (int16_t)cz;
+                    } else {
+                        atomicOr(out.err, kErrSegOverflow);
+                    }
                 }
                 po++;
                 pts++;
             };
+            auto step = [&](int s) {  // move the coordinates by the delta of scan index s
+                const int d = __shfl_sync(kFull, my_d, s);
+                cx += d % 3 - 1;
+                cy += (d / 3) % 3 - 1;
+                cz += d / 9 - 1;
+                return __shfl_sync(kFull, my_off, s);
+            };
+            const int v0p = V0[p];
             for (int br = 0; br < -vp; br++) {
-                int is_end = V0[p] > -2 && V0[p] < 2;
-                if (EMIT && lane == 0) out.start[so] = po;
-                put(p);
-                // first neighbour after ni in scan order with a nonzero value
-                const unsigned m = __ballot_sync(kFull, lane_ok && lane > ni && V[p + my_off] != 0);
+                int is_end = v0p > -2 && v0p < 2;
+                const int seg_rel = pts;
+                cx = p_x;
+                cy = p_y;
+                cz = p_z;
+                put();
+                // first neighbour after ni in scan order with a nonzero value;
+                // every lane loads its neighbour's current and original value
+                // at once, and the chosen one's reach the warp by shuffles
+                int vn = lane_ok ? V[p + my_off] : 0, v0n = lane_ok ? V0[p + my_off] : 0;
+                const unsigned m = __ballot_sync(kFull, lane_ok && lane > ni && vn != 0);
                 ni = m ? __ffs(m) - 1 : ND;
                 if (ni < ND) {
-                    long long t = p + __shfl_sync(kFull, my_off, ni);
+                    long long prev = p;
+                    int back = ND - 1 - ni;  // scan index of the step back to prev
+                    int vt = __shfl_sync(kFull, vn, ni), v0t = __shfl_sync(kFull, v0n, ni);
+                    long long t = p + step(ni);
+                    bool first = true, stall = false;
                     for (int guard = 0; guard < (1 << 30); guard++) {
-                        if (V[t] != 2) break;
+                        if (vt != 2) break;
+                        put();
+                        vn = lane_ok ? V[t + my_off] : 0;
+                        v0n = lane_ok ? V0[t + my_off] : 0;
+                        const unsigned m2 = __ballot_sync(kFull, lane_ok && lane != back && vn != 0);
+                        if (!m2) {
+                            stall = true;
+                            break;
+                        }
+                        if (lane == 0 && (first || v0t != 2)) V[t] = 0;
+                        const int s2 = __ffs(m2) - 1;
+                        prev = t;
+                        back = ND - 1 - s2;
+                        vt = __shfl_sync(kFull, vn, s2);
+                        v0t = __shfl_sync(kFull, v0n, s2);
+                        t += step(s2);
+                        first = false;
                         __syncwarp();
-                        if (lane == 0) V[t] = 0;
-                        __syncwarp();
-                        put(t);
-                        const unsigned m2 = __ballot_sync(kFull, lane_ok && V[t + my_off] != 0);
-                        if (m2) t += __shfl_sync(kFull, my_off, __ffs(m2) - 1);
                     }
-                    put(t);
-                    if (V0[t] > -2 && V0[t] < 2) is_end = 1;
                     __syncwarp();
-                    if (lane == 0) V[t] = (int8_t)(V[t] + 1);
+                    // the last chain pixel (prev, unless the walk never left p) becomes zero in memory too
+                    if (lane == 0 && prev != p) V[prev] = 0;
+                    __syncwarp();
+                    put();
+                    if (v0t > -2 && v0t < 2) is_end = 1;
+                    // a stalled walk stays on t, which the reference zeroed: it becomes 1
+                    if (lane == 0) V[t] = stall ? (int8_t)1 : (int8_t)(vt + 1);
                     __syncwarp();
                 }
-                if (EMIT && lane == 0) out.is_end[so] = (uint8_t)is_end;
+                if (lane == 0) {
+                    if (so < so_end) {
+                        out.trel[so] = seg_rel;
+                        out.tend[so] = (uint8_t)is_end;
+                    } else {
+                        atomicOr(out.err, kErrSegOverflow);
+                    }
+                }
                 so++;
                 segs++;
             }
-            if (!EMIT && lane == 0) {
+            if (lane == 0) {
                 out.nseg[rank] = segs;
                 out.npts[rank] = pts;
             }
+        }
+    }
+}
+
+// fg pixels per union-find root (the component's pixel count)
+__global__ void comp_px_kernel(const int8_t *__restrict__ V, uint32_t *par, long long n, uint32_t *cnt)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        if (V[i] != 0) atomicAdd(cnt + uf_find(par, (uint32_t)i), 1u);
+}
+
+// per component: branches = sum of |v| over its nodes (a bound on its
+// segments), pixels from its root
+__global__ void comp_sums_kernel(const int8_t *__restrict__ V0, const uint32_t *__restrict__ snodes,
+                                 const uint32_t *__restrict__ keys_s, const int *__restrict__ flag,
+                                 const int *__restrict__ fpos, const uint32_t *__restrict__ cnt, int nn,
+                                 int *branches, int *px)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        const int c = fpos[i] + flag[i] - 1;
+        atomicAdd(branches + c, -(int)V0[snodes[i]]);
+        if (flag[i]) px[c] = (int)cnt[keys_s[i]];
+    }
+}
+
+// bounds of a component's output: segments <= branches; points <= pixels +
+// 3 * branches (each branch adds its start and end point, and a pixel is
+// walked through again only after two walks ended on it)
+__global__ void comp_bounds_kernel(const int *__restrict__ branches, const int *__restrict__ px, int ncomp,
+                                   int *bpts, int *bsegs)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncomp; c += gridDim.x * blockDim.x) {
+        bpts[c] = c < ncomp ? px[c] + 3 * branches[c] : 0;
+        bsegs[c] = c < ncomp ? branches[c] : 0;
+    }
+}
+
+// Move each node's output from its component's temporary range to its place
+// in the reference's emission order (one warp per node).
+template <int DIMS>
+__global__ void place_kernel(const WalkOut w, const int *__restrict__ seg_off, const int *__restrict__ pt_off,
+                             int nn, int32_t *start, uint8_t *is_end, int16_t *px, int16_t *py, int16_t *pz)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nn; r += warps) {
+        const int np = w.npts[r], ns = w.nseg[r];
+        const int ti = w.tpo[r], to = pt_off[r], si = w.tso[r], so = seg_off[r];
+        for (int j = lane; j < np; j += 32) {
+            px[to + j] = w.tx[ti + j];
+            py[to + j] = w.ty[ti + j];
+            if (DIMS == 3) pz[to + j] = w.tz[ti + j];
+        }
+        for (int j = lane; j < ns; j += 32) {
+            start[so + j] = to + w.trel[si + j];
+            is_end[so + j] = w.tend[si + j];
         }
     }
 }
@@ -413,24 +540,66 @@ int segments_device_arrays(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, i
     // sorted node raster indices nodes[rank_s[k]] (keys are no longer needed)
     uint32_t *snodes = keys;
     gather_kernel<<<grid_of(nn), 256, 0, st>>>(nodes, rank_s, snodes, nn);
-    // walk 1: count segments and points per start node
+    // bounds of every component's output, and its temporary ranges
+    void *p23, *p24, *p26;
+    if ((rc = ctx_scratch(c, 23, (size_t)npx * 4, &p23)) ||
+        (rc = ctx_scratch(c, 24, (size_t)(ncomp + 1) * 6 * 4, &p24)) ||
+        (rc = ctx_scratch(c, 26, (size_t)(nn + 1) * 2 * 4, &p26)))
+        return rc;
+    uint32_t *pxcnt = (uint32_t *)p23;
+    int *branches = (int *)p24, *cpx = branches + (ncomp + 1), *bpts = cpx + (ncomp + 1),
+        *bsegs = bpts + (ncomp + 1), *cpb = bsegs + (ncomp + 1), *csb = cpb + (ncomp + 1);
+    cudaMemsetAsync(pxcnt, 0, (size_t)npx * 4, st);
+    cudaMemsetAsync(branches, 0, (size_t)(ncomp + 1) * 4, st);
+    comp_px_kernel<<<grid_of(npx), 256, 0, st>>>(V, par, npx, pxcnt);
+    comp_sums_kernel<<<grid_of(nn), 256, 0, st>>>(V0, snodes, keys_s, flag, fpos, pxcnt, nn, branches, cpx);
+    comp_bounds_kernel<<<grid_of(ncomp + 1), 256, 0, st>>>(branches, cpx, ncomp, bpts, bsegs);
+    if ((e = exscan(c, 14, bpts, cpb, ncomp + 1, st)) != cudaSuccess ||
+        (e = exscan(c, 14, bsegs, csb, ncomp + 1, st)) != cudaSuccess)
+        return cuda_fail(e, "component bounds scan");
+    int tb[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(&tb[0], cpb + ncomp, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&tb[1], csb + ncomp, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_fail(e, "component bounds");
+    if (tb[0] < 0 || tb[1] < 0) return fail(BGT_ERR_LIMIT, "segment output bound exceeds 2^31 entries");
+    const size_t Tp = (size_t)tb[0], Ts = (size_t)tb[1];
+    const size_t t_x = 0, t_y = align16(Tp * 2 + 2), t_z = t_y + align16(Tp * 2 + 2), t_rel = t_z + align16(Tp * 2 + 2),
+                 t_end = t_rel + align16(Ts * 4 + 4), t_err = t_end + align16(Ts + 1), t_tot = t_err + 16;
+    void *p25;
+    if ((rc = ctx_scratch(c, 25, t_tot, &p25))) return rc;
+    char *tbuf = (char *)p25;
     WalkOut wo{};
     wo.nseg = nseg;
     wo.npts = npts;
+    wo.tpo = (int *)p26;
+    wo.tso = wo.tpo + (nn + 1);
+    wo.cpb = cpb;
+    wo.csb = csb;
+    wo.tx = (int16_t *)(tbuf + t_x);
+    wo.ty = (int16_t *)(tbuf + t_y);
+    wo.tz = (int16_t *)(tbuf + t_z);
+    wo.trel = (int32_t *)(tbuf + t_rel);
+    wo.tend = (uint8_t *)(tbuf + t_end);
+    wo.err = (int *)(tbuf + t_err);
+    cudaMemsetAsync(wo.err, 0, 4, st);
+    // one walk over every component (a warp each), outputs in emission order per component
     const int wgrid = (int)std::min<long long>(((long long)ncomp * 32 + 255) / 256, 148LL * 16);
     if (dims == 2)
-        walk_kernel<2, false><<<wgrid, 256, 0, st>>>(V, V0, W, H, snodes, rank_s, cstart, ncomp, nn, wo);
+        walk_kernel<2><<<wgrid, 256, 0, st>>>(V, V0, W, H, snodes, rank_s, cstart, ncomp, nn, wo);
     else
-        walk_kernel<3, false><<<wgrid, 256, 0, st>>>(V, V0, W, H, snodes, rank_s, cstart, ncomp, nn, wo);
+        walk_kernel<3><<<wgrid, 256, 0, st>>>(V, V0, W, H, snodes, rank_s, cstart, ncomp, nn, wo);
     cudaMemsetAsync(nseg + nn, 0, 4, st);
     cudaMemsetAsync(npts + nn, 0, 4, st);
     if ((e = exscan(c, 14, nseg, seg_off, nn + 1, st)) != cudaSuccess) return cuda_fail(e, "segment scan");
     if ((e = exscan(c, 14, npts, pt_off, nn + 1, st)) != cudaSuccess) return cuda_fail(e, "point scan");
-    int tot[2] = {0, 0};
+    int tot[3] = {0, 0, 0};
     if ((e = cudaMemcpyAsync(&tot[0], seg_off + nn, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(&tot[1], pt_off + nn, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&tot[2], wo.err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return cuda_fail(e, "segment totals");
+    if (tot[2]) return fail(BGT_ERR_LIMIT, "segment output outgrew its bound");
     const int S = tot[0], Np = tot[1];
     // output block: start[S+1] int32, is_end[S] u8, px, py (pz) int16[Np]
     const size_t o_start = 0, o_end = align16((size_t)(S + 1) * 4), o_px = o_end + align16((size_t)S + 1),
@@ -439,27 +608,22 @@ int segments_device_arrays(bgt_ctx *c, int dims, const uint32_t *d_buf, int W, i
     void *p19;
     if ((rc = ctx_scratch(c, 19, o_tot, &p19))) return rc;
     char *ob = (char *)p19;
-    wo.seg_off = seg_off;
-    wo.pt_off = pt_off;
-    wo.start = (int32_t *)(ob + o_start);
-    wo.is_end = (uint8_t *)(ob + o_end);
-    wo.px = (int16_t *)(ob + o_px);
-    wo.py = (int16_t *)(ob + o_py);
-    wo.pz = (int16_t *)(ob + o_pz);
-    // walk 2 from the original values: write every segment at its final place
-    cudaMemcpyAsync(V, V0, npx, cudaMemcpyDeviceToDevice, st);
+    int32_t *o_st = (int32_t *)(ob + o_start);
+    uint8_t *o_ie = (uint8_t *)(ob + o_end);
+    int16_t *o_x = (int16_t *)(ob + o_px), *o_y = (int16_t *)(ob + o_py), *o_z = (int16_t *)(ob + o_pz);
+    const int pgrid = (int)std::min<long long>(((long long)nn * 32 + 255) / 256, 148LL * 16);
     if (dims == 2)
-        walk_kernel<2, true><<<wgrid, 256, 0, st>>>(V, V0, W, H, snodes, rank_s, cstart, ncomp, nn, wo);
+        place_kernel<2><<<pgrid, 256, 0, st>>>(wo, seg_off, pt_off, nn, o_st, o_ie, o_x, o_y, o_z);
     else
-        walk_kernel<3, true><<<wgrid, 256, 0, st>>>(V, V0, W, H, snodes, rank_s, cstart, ncomp, nn, wo);
-    cudaMemcpyAsync(wo.start + S, pt_off + nn, 4, cudaMemcpyDeviceToDevice, st);
+        place_kernel<3><<<pgrid, 256, 0, st>>>(wo, seg_off, pt_off, nn, o_st, o_ie, o_x, o_y, o_z);
+    cudaMemcpyAsync(o_st + S, pt_off + nn, 4, cudaMemcpyDeviceToDevice, st);
     out->nseg = S;
     out->npts = Np;
-    out->start = wo.start;
-    out->is_end = wo.is_end;
-    out->px = wo.px;
-    out->py = wo.py;
-    out->pz = dims == 3 ? wo.pz : nullptr;
+    out->start = o_st;
+    out->is_end = o_ie;
+    out->px = o_x;
+    out->py = o_y;
+    out->pz = dims == 3 ? o_z : nullptr;
     return BGT_OK;
 }
 

@@ -59,6 +59,7 @@ def parse():
                    help="tile configurations: cached autotuner table (tune when absent), retune, or defaults")
     p.add_argument("--e2e-chunks", type=int, default=4, help="pipeline depth of the host-to-host leg")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-centerline", action="store_true", help="skip the CenterlineExtraction timing block")
     p.add_argument("--serve-seconds", type=float, default=4.0, help="measured seconds of the serving run")
     return p.parse_args()
 
@@ -404,7 +405,43 @@ def run_bgt(args, rank, world, local):
                 "offered_requests_per_s": s["offered_rate_per_s"], "measured_seconds": s["duration_s"],
                 "latency": "submission to output in pinned host memory",
             }
+        if not args.no_centerline:
+            line["centerline"] = centerline_block()
     return line
+
+
+def centerline_block(calls: int = 10) -> dict:
+    """The reference-facing CenterlineExtraction call (host buffers in and
+    out: H2D, thinning, device segments, device pruning/smoothing/CSR, D2H)
+    on the 512x512 stroke frame and the 256^3 tree volume, timed per call
+    beside the reference's own CPU CenterlineExtraction (its .cpp code and
+    rules, oracle/_ref) on the same inputs; the outputs are compared."""
+    import numpy as np
+    from begputhinning_b200 import CenterlineExtraction, synth
+    from begputhinning_b200.api import dtype_code
+    from oracle import pyoracle as po
+    ml, sp = 10, 3
+    out = {"max_segment_length": ml, "smoothing_span": sp}
+    for name, data in (("frame_512x512", synth.frame512(0)), ("volume_256x256x256", synth.trees256(2))):
+        res = CenterlineExtraction(data, ml, sp)  # warm-up (allocations, tuning of the single-instance batch)
+        ts = []
+        for _ in range(calls):
+            t0 = time.perf_counter()
+            res = CenterlineExtraction(data, ml, sp)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        ms = statistics.median(ts)
+        entry = {"ms_per_call": ms, "mvoxel_per_s": data.size / ms / 1e3, "segments": int(len(res[-1]) - 1)}
+        if po.have_ref("2d" if data.ndim == 2 else "3d"):
+            t0 = time.perf_counter()
+            ref = (po.ref_centerline2d if data.ndim == 2 else po.ref_centerline3d)(data, dtype_code(data.dtype), ml, sp)
+            rms = (time.perf_counter() - t0) * 1e3
+            same = np.array_equal(res[-1], ref.idx) and all(
+                np.array_equal(a.view(np.uint32), b.view(np.uint32))
+                for a, b in zip(res[:-1], [ref.x, ref.y] + ([ref.z] if data.ndim == 3 else [])))
+            entry.update({"reference_cpu_ms_per_call": rms, "identical_to_reference": bool(same),
+                          "speedup_vs_reference_cpu": rms / ms})
+        out[name] = entry
+    return out
 
 
 def run_reference(args, rank, world):
