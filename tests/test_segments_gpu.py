@@ -96,3 +96,25 @@ def test_centerline_config0(ctx):
     assert np.array_equal(idx, ref.idx)
     assert np.array_equal(x.view(np.uint32), ref.x.view(np.uint32))
     assert np.array_equal(y.view(np.uint32), ref.y.view(np.uint32))
+
+
+def test_segments_pixel_walk_path(ctx, monkeypatch):
+    """The per-component pixel walk (the fallback of the node-parallel walk)
+    against the oracle, on thinned images, raw masks and volumes."""
+    from begputhinning_b200 import ExtractSegmentsV
+    monkeypatch.setenv("BGT_SEGMENTS_PIXEL_WALK", "1")
+    rng = np.random.default_rng(24)
+    cases = _thin_cases2d()[:6] + [random2d(rng, 45, 52, 0.4)]
+    for k, img in enumerate(cases):
+        assert ExtractSegmentsV(img, ctx).as_lists() == po.segments2d(img).as_lists(), f"case {k}"
+    vol = blobs3d(rng, 20, 24, 28, 4)
+    for v in (po.thin3d(vol)[0], vol):
+        assert ExtractSegmentsV(v, ctx).as_lists() == po.segments3d(v).as_lists()
+
+
+def test_segments_large_images(ctx):
+    """Stroke networks large enough that one component spans the image."""
+    from begputhinning_b200 import ExtractSegmentsV, Thinning2D, synth
+    for w, n in [(700, 22), (1100, 50)]:
+        img = Thinning2D(synth.strokes2d(9, w, w, n))
+        assert ExtractSegmentsV(img, ctx).as_lists() == po.segments2d(img).as_lists()
