@@ -516,6 +516,13 @@ static int upload_io(bgt_batch *b)
         io[i].inst = i;
         io[i].wbegin = w;
         io[i].gbegin = g;
+        io[i].dP = make_fastdiv((uint32_t)in.P);
+        io[i].dH = make_fastdiv((uint32_t)in.H);
+        io[i].dW = make_fastdiv((uint32_t)in.W);
+        io[i].dWW = make_fastdiv((uint32_t)((in.W + 31) / 32));
+        io[i].dTW = make_fastdiv((uint32_t)in.TW);
+        io[i].dTH = make_fastdiv((uint32_t)in.TH);
+        io[i].dTZ = make_fastdiv((uint32_t)std::max(1, in.TZ));
         w += (long long)in.P * in.H * in.D;
         if (dtype_size(s.dtype) == 1 && s.out) {
             // unpack unit: 16-byte-aligned chunk of the output

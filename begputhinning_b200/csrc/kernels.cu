@@ -358,13 +358,40 @@ __device__ __forceinline__ uint32_t bytes4_to_bits(uint32_t cmp)
     return ((cmp & 0x80808080u) * 0x00204081u) >> 28;
 }
 
+// 32 bytes at word offset Q (0..3) and byte shift sh of 12 loaded words ->
+// 32 "nonzero" bits
+template <int Q>
+__device__ __forceinline__ uint32_t pack_from12(const uint32_t (&u)[12], unsigned sh)
+{
+    uint32_t w = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) w |= bytes4_to_bits(__vcmpne4(__funnelshift_r(u[Q + k], u[Q + k + 1], sh), 0u)) << (4 * k);
+    return w;
+}
+
 // `room` = bytes readable from p onward (>= 36 allows the aligned 4-byte
-// loads that cover p .. p+31 whatever p's alignment).
+// loads that cover p .. p+31 whatever p's alignment); `lead` = bytes readable
+// before p (>= 15 and room >= 33 allow three 16-byte loads from the 16-byte
+// boundary at or below p).
 template <typename T, int MODE>
-__device__ __forceinline__ uint32_t pack_word(const T *p, int n, long long room = 0)
+__device__ __forceinline__ uint32_t pack_word(const T *p, int n, long long room = 0, long long lead = 0)
 {
     if constexpr (sizeof(T) == 1 && (MODE != 1 || std::is_unsigned<T>::value || std::is_same<T, bool>::value)) {
         // one-byte types whose test is "nonzero" (2D rule and unsigned/bool 3D rule)
+        const uintptr_t pa = reinterpret_cast<uintptr_t>(p);
+        if (n == 32 && (long long)(pa & 15u) <= lead && (long long)(48 - (pa & 15u)) <= room) {
+            // three aligned 16-byte loads cover p .. p+31; realign by words and bytes
+            const uint4 *a16 = reinterpret_cast<const uint4 *>(pa & ~uintptr_t(15));
+            const uint4 A = __ldg(a16), B = __ldg(a16 + 1), C = __ldg(a16 + 2);
+            const uint32_t u[12] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w};
+            const unsigned sh = (unsigned)(pa & 3u) * 8u;
+            switch ((pa >> 2) & 3u) {
+            case 0: return pack_from12<0>(u, sh);
+            case 1: return pack_from12<1>(u, sh);
+            case 2: return pack_from12<2>(u, sh);
+            default: return pack_from12<3>(u, sh);
+            }
+        }
         if (n == 32 && (reinterpret_cast<uintptr_t>(p) & 15u) == 0) {
             const uint4 a = *reinterpret_cast<const uint4 *>(p);
             const uint4 b = *reinterpret_cast<const uint4 *>(p + 16);
@@ -404,10 +431,10 @@ __device__ __forceinline__ uint32_t pack_word(const T *p, int n, long long room 
 }
 
 template <typename T>
-__device__ __forceinline__ uint32_t pack_word_mode(const T *p, int n, int mode, long long room)
+__device__ __forceinline__ uint32_t pack_word_mode(const T *p, int n, int mode, long long room, long long lead = 0)
 {
-    return mode == 0 ? pack_word<T, 0>(p, n, room) : mode == 1 ? pack_word<T, 1>(p, n, room)
-                                                               : pack_word<T, 2>(p, n, room);
+    return mode == 0 ? pack_word<T, 0>(p, n, room, lead) : mode == 1 ? pack_word<T, 1>(p, n, room, lead)
+                                                                     : pack_word<T, 2>(p, n, room, lead);
 }
 
 __device__ __forceinline__ int dtype_bytes(int dtype)
@@ -430,8 +457,13 @@ __device__ __forceinline__ int find_io(const IODesc *io, int n, long long g, boo
 __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__restrict__ io, int n,
                                 long long total)
 {
+    // the instance's descriptor, cached while consecutive units stay in it
     int k = -1;
     long long kb = 0, ke = 0;
+    IODesc d{};
+    uint32_t *buf0 = nullptr, *buf1 = nullptr;
+    int *lc = nullptr;
+    int P = 0, H = 0, tiles_x = 0, tiles_y = 0;
     // each block takes one contiguous range, so consecutive units of a thread
     // stay in the same instance and the instance lookup is rarely repeated
     const long long per = (total + gridDim.x - 1) / gridDim.x;
@@ -439,43 +471,53 @@ __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__
     for (long long g = per * blockIdx.x + threadIdx.x; g < g_end; g += blockDim.x) {
         if (g < kb || g >= ke) {  // instance lookup only when leaving the cached range
             k = find_io(io, n, g, false);
-            kb = io[k].wbegin;
+            d = io[k];
+            kb = d.wbegin;
             ke = k + 1 < n ? io[k + 1].wbegin : total;
+            const Inst &in = insts[d.inst];
+            buf0 = in.buf[0];
+            buf1 = in.buf[1];
+            lc = in.lc;
+            P = in.P;
+            H = in.H;
+            tiles_x = in.tiles_x;
+            tiles_y = in.tiles_y;
         }
-        const IODesc &d = io[k];
-        const Inst &in = insts[d.inst];
         // 32-bit index math: an instance has fewer than 2^31 packed words
-        const unsigned i = (unsigned)(g - d.wbegin);
-        const unsigned row = i / (unsigned)in.P;
-        const int j = (int)(i - row * (unsigned)in.P);
-        const int z = (int)(row / (unsigned)in.H), y = (int)(row - (unsigned)z * (unsigned)in.H);
+        const uint32_t i = (uint32_t)(g - kb);
+        const uint32_t row = fdiv(d.dP, i);
+        const int j = (int)(i - row * (uint32_t)P);
+        const uint32_t z = fdiv(d.dH, row);
+        const int y = (int)(row - z * (uint32_t)H);
         const int x0 = j * 32;
         uint32_t w = 0;
-        if (x0 < d.inW && y < d.inH && z < d.inD) {
+        if (x0 < d.inW && y < d.inH && (int)z < d.inD) {
             const long long off = ((long long)z * d.inH + y) * (long long)d.inW + x0;
             const int cnt = min(32, d.inW - x0);
             // elements from off to the end of the input; words that start in the
             // first 3 bytes of an unaligned input are kept on the scalar path
             const bool head_ok = off >= 4 || (reinterpret_cast<uintptr_t>(d.in) & 3u) == 0;
             const long long room = head_ok ? (long long)d.inW * d.inH * d.inD - off : 0;
+            const long long lead = off;  // one-byte inputs: bytes before this word's first pixel
             switch (d.dtype) {
-            case BGT_U8: w = pack_word_mode((const uint8_t *)d.in + off, cnt, d.mode, room); break;
-            case BGT_I8: w = pack_word_mode((const int8_t *)d.in + off, cnt, d.mode, room); break;
-            case BGT_CHAR: w = pack_word_mode((const char *)d.in + off, cnt, d.mode, room); break;
+            case BGT_U8: w = pack_word_mode((const uint8_t *)d.in + off, cnt, d.mode, room, lead); break;
+            case BGT_I8: w = pack_word_mode((const int8_t *)d.in + off, cnt, d.mode, room, lead); break;
+            case BGT_CHAR: w = pack_word_mode((const char *)d.in + off, cnt, d.mode, room, lead); break;
             case BGT_U16: w = pack_word_mode((const uint16_t *)d.in + off, cnt, d.mode, room); break;
             case BGT_I16: w = pack_word_mode((const int16_t *)d.in + off, cnt, d.mode, room); break;
             case BGT_U32: w = pack_word_mode((const uint32_t *)d.in + off, cnt, d.mode, room); break;
             case BGT_I32: w = pack_word_mode((const int32_t *)d.in + off, cnt, d.mode, room); break;
             case BGT_F32: w = pack_word_mode((const float *)d.in + off, cnt, d.mode, room); break;
             case BGT_F64: w = pack_word_mode((const double *)d.in + off, cnt, d.mode, room); break;
-            default: w = pack_word_mode((const bool *)d.in + off, cnt, d.mode, room); break;
+            default: w = pack_word_mode((const bool *)d.in + off, cnt, d.mode, room, lead); break;
             }
         }
-        in.buf[0][i] = w;
-        in.buf[1][i] = w;
+        buf0[i] = w;
+        buf1[i] = w;
         if (w) {  // tile holds foreground: lc = -1 (pre-filled with kNever)
-            const int t = ((z / in.TZ) * in.tiles_y + y / in.TH) * in.tiles_x + j / in.TW;
-            in.lc[t] = -1;
+            const int t = ((int)fdiv(d.dTZ, z) * tiles_y + (int)fdiv(d.dTH, (uint32_t)y)) * tiles_x +
+                          (int)fdiv(d.dTW, (uint32_t)j);
+            lc[t] = -1;
         }
     }
 }
@@ -514,44 +556,56 @@ __device__ __forceinline__ void unpack_word(uint32_t w, T *o, int n)
     for (int b = 0; b < n; b++) o[b] = (T)((w >> b) & 1u);
 }
 
+// 16 consecutive bits of a packed row starting at pixel x (x + 16 <= the
+// row's words * 32), as the low half of a word.
+__device__ __forceinline__ uint32_t row_bits16(const uint32_t *r, int x)
+{
+    const uint32_t w0 = __ldg(r + (x >> 5));
+    const uint32_t w1 = (x & 31) > 16 ? __ldg(r + (x >> 5) + 1) : 0u;
+    return __funnelshift_r(w0, w1, x & 31) & 0xffffu;
+}
+
 // One-byte outputs: unit = one 16-byte-aligned chunk of the output (absolute
 // address), written with one 128-bit store when the chunk lies inside the
 // instance's output, bytewise at its two ends.  Each byte is pixel
-// (row, x) of the flat index; rows may change inside a chunk.
-__device__ __forceinline__ void unpack_chunk16(const Inst &in, const IODesc &d, long long c)
+// (row, x) of the flat index; a chunk spans at most two rows when W >= 16.
+__device__ __forceinline__ void unpack_chunk16(const uint32_t *buf, int W, int P, long long n, const IODesc &d,
+                                               long long c)
 {
     const uintptr_t out = reinterpret_cast<uintptr_t>(d.out);
-    const long long n = (long long)in.W * in.H * in.D;
     const uintptr_t a = (out & ~uintptr_t(15)) + (uintptr_t)c * 16u;
     const long long lo = (long long)(a > out ? a - out : 0);  // first flat index in the chunk
     const long long hi = min((long long)(a + 16 - out), n);   // one past the last
     // flat indices of one instance stay below 2^31 (sizes are capped at 32767
     // per axis and the batch limits an instance to < 2^31 pixels)
-    unsigned row = (unsigned)lo / (unsigned)in.W;
-    int x = (int)((unsigned)lo - row * (unsigned)in.W);
-    if (hi - lo == 16 && a >= out && x + 16 <= in.W) {
-        // whole chunk inside one row: 16 consecutive bits, expanded 4 at a time
-        const uint32_t *r = in.buf[0] + (size_t)row * in.P;
-        const uint32_t w0 = __ldcg(r + (x >> 5));
-        const uint32_t w1 = ((x & 31) > 16) ? __ldcg(r + (x >> 5) + 1) : 0u;
-        const uint32_t bits = __funnelshift_r(w0, w1, x & 31);
+    uint32_t row = fdiv(d.dW, (uint32_t)lo);
+    int x = (int)((uint32_t)lo - row * (uint32_t)W);
+    if (hi - lo == 16 && a >= out && W >= 16) {
+        uint32_t bits;
+        if (x + 16 <= W) {
+            bits = row_bits16(buf + (size_t)row * P, x);
+        } else {  // the chunk runs into the next row
+            const int n0 = W - x;
+            bits = (row_bits16(buf + (size_t)row * P, x) & ((1u << n0) - 1u)) |
+                   (row_bits16(buf + (size_t)(row + 1) * P, 0) << n0);
+        }
         *reinterpret_cast<uint4 *>(a) = make_uint4(bits4_to_bytes(bits & 15u), bits4_to_bytes((bits >> 4) & 15u),
                                                    bits4_to_bytes((bits >> 8) & 15u),
                                                    bits4_to_bytes((bits >> 12) & 15u));
         return;
     }
-    uint32_t word = __ldcg(in.buf[0] + (size_t)row * in.P + (x >> 5));
+    uint32_t word = __ldg(buf + (size_t)row * P + (x >> 5));
     uint32_t bytes[4] = {0u, 0u, 0u, 0u};
     const int first = (int)((out + lo) - a);  // byte position of flat index lo in the chunk
     for (long long f = lo; f < hi; f++) {
         const int pos = first + (int)(f - lo);
         bytes[pos >> 2] |= ((word >> (x & 31)) & 1u) << (8 * (pos & 3));
-        if (++x == in.W) {
+        if (++x == W) {
             x = 0;
             row++;
-            if (f + 1 < hi) word = __ldcg(in.buf[0] + (size_t)row * in.P);
+            if (f + 1 < hi) word = __ldg(buf + (size_t)row * P);
         } else if ((x & 31) == 0 && f + 1 < hi) {
-            word = __ldcg(in.buf[0] + (size_t)row * in.P + (x >> 5));
+            word = __ldg(buf + (size_t)row * P + (x >> 5));
         }
     }
     if (first == 0 && hi - lo == 16) {
@@ -567,6 +621,11 @@ __global__ void unpack_all_kernel(const Inst *__restrict__ insts, const IODesc *
 {
     int k = -1;
     long long kb = 0, ke = 0;
+    IODesc d{};
+    const uint32_t *buf = nullptr;
+    int W = 0, P = 0, wwords = 0;
+    long long npx = 0;
+    bool bytes1 = false;
     // each block takes one contiguous range, so consecutive units of a thread
     // stay in the same instance and the instance lookup is rarely repeated
     const long long per = (total + gridDim.x - 1) / gridDim.x;
@@ -574,34 +633,36 @@ __global__ void unpack_all_kernel(const Inst *__restrict__ insts, const IODesc *
     for (long long g = per * blockIdx.x + threadIdx.x; g < g_end; g += blockDim.x) {
         if (g < kb || g >= ke) {  // instance lookup only when leaving the cached range
             k = find_io(io, n, g, true);
-            kb = io[k].gbegin;
+            d = io[k];
+            kb = d.gbegin;
             ke = k + 1 < n ? io[k + 1].gbegin : total;
+            const Inst &in = insts[d.inst];
+            buf = in.buf[0];
+            W = in.W;
+            P = in.P;
+            wwords = (in.W + 31) >> 5;
+            npx = (long long)in.W * in.H * in.D;
+            bytes1 = dtype_bytes(d.dtype) == 1;
         }
-        const IODesc &d = io[k];
         if (!d.out) continue;
-        const Inst &in = insts[d.inst];
-        if (dtype_bytes(d.dtype) == 1) {
-            unpack_chunk16(in, d, g - d.gbegin);
+        if (bytes1) {
+            unpack_chunk16(buf, W, P, npx, d, g - kb);
             continue;
         }
-        const int wwords = (in.W + 31) >> 5;
-        const long long i = g - d.gbegin;
-        const long long row = i / wwords;
-        const int j = (int)(i - row * wwords);
-        const uint32_t w = __ldcg(in.buf[0] + row * in.P + j);
-        const long long off = row * (long long)in.W + (long long)j * 32;
-        const int cnt = min(32, in.W - j * 32);
+        const uint32_t i = (uint32_t)(g - kb);
+        const uint32_t row = fdiv(d.dWW, i);
+        const int j = (int)(i - row * (uint32_t)wwords);
+        const uint32_t w = __ldg(buf + (size_t)row * P + j);
+        const long long off = (long long)row * W + (long long)j * 32;
+        const int cnt = min(32, W - j * 32);
         switch (d.dtype) {
-        case BGT_U8: unpack_word(w, (uint8_t *)d.out + off, cnt); break;
-        case BGT_I8: unpack_word(w, (int8_t *)d.out + off, cnt); break;
-        case BGT_CHAR: unpack_word(w, (char *)d.out + off, cnt); break;
         case BGT_U16: unpack_word(w, (uint16_t *)d.out + off, cnt); break;
         case BGT_I16: unpack_word(w, (int16_t *)d.out + off, cnt); break;
         case BGT_U32: unpack_word(w, (uint32_t *)d.out + off, cnt); break;
         case BGT_I32: unpack_word(w, (int32_t *)d.out + off, cnt); break;
         case BGT_F32: unpack_word(w, (float *)d.out + off, cnt); break;
         case BGT_F64: unpack_word(w, (double *)d.out + off, cnt); break;
-        default: unpack_word(w, (bool *)d.out + off, cnt); break;
+        default: break;  // one-byte types take the chunk path above
         }
     }
 }

@@ -46,6 +46,32 @@ struct Sched {
 };
 
 // Per-instance input/output of a batch-wide pack/unpack launch.
+// Unsigned 32-bit division by a divisor fixed per instance, as a multiply
+// and shifts (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", 1994, section 4): with l = ceil(log2 d),
+// m = floor(2^32 (2^l - d) / d) + 1, t = mulhi(m, n):
+// n / d = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0), exact for every
+// 32-bit n.
+struct FastDiv {
+    uint32_t m = 1, s1 = 0, s2 = 0, d = 1;
+};
+inline FastDiv make_fastdiv(uint32_t d)
+{
+    FastDiv f;
+    f.d = d;
+    uint32_t l = 0;
+    while (l < 32 && (1ull << l) < d) l++;
+    f.m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+    f.s1 = l < 1 ? l : 1;
+    f.s2 = l > 1 ? l - 1 : 0;
+    return f;
+}
+__device__ __forceinline__ uint32_t fdiv(const FastDiv &f, uint32_t n)
+{
+    const uint32_t t = __umulhi(f.m, n);
+    return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
 struct alignas(16) IODesc {
     const void *in;
     void *out;
@@ -54,6 +80,9 @@ struct alignas(16) IODesc {
     int inst;                // instance index
     long long wbegin;        // first global packed-word index of the instance (pack)
     long long gbegin;        // first global unpack-word index (rows x ceil(W/32))
+    // dividers of the instance: words per row P, rows H, pixels per row W,
+    // used words per row ceil(W/32), and the core tile extents TW, TH, TZ
+    FastDiv dP, dH, dW, dWW, dTW, dTH, dTZ;
 };
 
 // Launchers (stream-ordered, no host synchronisation).
