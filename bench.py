@@ -27,6 +27,7 @@ no collective is on the data path (weak scaling).
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -47,7 +48,7 @@ WORKLOAD = ("mixed batch: 512 2D stroke images, sides log-uniform 64-2048 (aspec
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="bgt", choices=["bgt", "reference"])
     p.add_argument("--seed", type=int, default=3)
@@ -79,9 +80,11 @@ def host_cores() -> int:
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples every 200 ms during the timed region."""
+    """nvidia-smi clock / throttle-reason samples every 100 ms; only the samples
+    whose timestamps fall inside the timed region (mark_start .. mark_end)
+    are summarised."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -89,12 +92,19 @@ class ClockSampler:
         self.gpu_id = gpu_id
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        self.t0 = datetime.datetime.now()
+
+    def mark_end(self):
+        self.t1 = datetime.datetime.now()
 
     def start(self):
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
-            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
             if self.gpu_id:
                 cmd += ["-i", self.gpu_id]
             self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
@@ -110,23 +120,27 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+                rows.append((ts, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
         os.unlink(self.path)
+        inside = [r for r in rows if self.t0 and self.t1 and self.t0 <= r[0] <= self.t1]
+        window = "timed region"
+        if not inside:  # timed region shorter than the sampling period
+            inside, window = rows, "timed region and the 0.3 s before it (region shorter than one sample period)"
+        sm = [r[1] for r in inside]
+        smax = [r[2] for r in inside]
+        reasons = {n for r in inside for n, v in zip(names, r[3]) if v.lower() == "active"}
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 def measured_peaks():
@@ -256,12 +270,14 @@ def run_bgt(args, rank, world, local):
     clocks.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark_start()
     with torch.cuda.stream(stream):
         e0.record(stream)
         for _ in range(args.steps):
             step()
         e1.record(stream)
     torch.cuda.synchronize()
+    clocks.mark_end()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
@@ -472,7 +488,7 @@ def run_reference(args, rank, world):
         sample.append(k)
         if time.perf_counter() - t0 > 1.5:
             break
-    budget = max(1.0, 150.0 / max(1, args.steps + args.warmup))  # seconds per step
+    budget = max(0.2, 120.0 / max(1, args.steps + args.warmup))  # seconds per step
     rate = sum(items[k].size for k in sample) / (time.perf_counter() - t0)
     target = rate * budget
     sample, vox = [], 0
@@ -515,8 +531,6 @@ def main():
         if line is not None:
             print(json.dumps(line), flush=True)
         return
-    import datetime
-
     import torch
     import torch.distributed as dist
     if world > 1:
