@@ -335,11 +335,19 @@ class PipelinedBatch:
     stream once its copy finished, and copied out on a third stream, so the
     copy-in of later groups and the copy-out of earlier ones run during the
     thinning of the current group.  Put instances with long chains of passes
-    (3D volumes) first: their group starts first."""
+    (3D volumes) first: their group starts first.
 
-    def __init__(self, shapes, chunks: int = 4, device: int = 0):
+    `buffers` device copies of the inputs and outputs are used in turn by
+    consecutive passes, so the copy-in of pass k+1 runs while pass k is still
+    being thinned and copied out (host-to-device and device-to-host copies
+    use the two directions of the link at the same time).  A device buffer is
+    overwritten only after the copy-out of the pass that last used it."""
+
+    def __init__(self, shapes, chunks: int = 4, device: int = 0, buffers: int = 2):
         import numpy as np
         import torch
+        if buffers < 1:
+            raise ValueError("buffers must be >= 1")
         self.device = device
         self.dev = torch.device("cuda", device)
         self.shapes = [tuple(s) for s in shapes]
@@ -356,32 +364,56 @@ class PipelinedBatch:
         if start < len(sizes):
             bounds.append((start, len(sizes)))
         self.groups = bounds
-        self.dev_in = torch.empty(self.total, dtype=torch.uint8, device=self.dev)
-        self.dev_out = torch.empty(self.total, dtype=torch.uint8, device=self.dev)
         self.s_in = torch.cuda.Stream(self.dev)
         self.s_comp = torch.cuda.Stream(self.dev)
         self.s_out = torch.cuda.Stream(self.dev)
         self.ctx = Context(device)
         self.ctx.set_stream(self.s_comp)
-        self.batches = []
-        for a, b in self.groups:
-            bt = Batch(self.ctx)
-            ids = [bt.add(self.shapes[i]) for i in range(a, b)]
-            bt.finalize()
-            for j, i in zip(ids, range(a, b)):
-                lo, hi = int(self.offs[i]), int(self.offs[i + 1])
-                bt.set_io(j, self.dev_in[lo:hi], self.dev_out[lo:hi])
-            self.batches.append(bt)
+        self.sets = []  # per device buffer: (dev_in, dev_out, batches)
+        for _ in range(buffers):
+            dev_in = torch.empty(self.total, dtype=torch.uint8, device=self.dev)
+            dev_out = torch.empty(self.total, dtype=torch.uint8, device=self.dev)
+            batches = []
+            for a, b in self.groups:
+                bt = Batch(self.ctx)
+                ids = [bt.add(self.shapes[i]) for i in range(a, b)]
+                bt.finalize()
+                for j, i in zip(ids, range(a, b)):
+                    lo, hi = int(self.offs[i]), int(self.offs[i + 1])
+                    bt.set_io(j, dev_in[lo:hi], dev_out[lo:hi])
+                batches.append(bt)
+            self.sets.append((dev_in, dev_out, batches))
+        self.free = [None] * buffers  # event: the set's last copy-out finished
+        self.turn = 0
         torch.cuda.synchronize(self.dev)
 
+    @property
+    def dev_in(self):
+        return self.sets[0][0]
+
+    @property
+    def dev_out(self):
+        return self.sets[0][1]
+
+    @property
+    def batches(self):
+        return self.sets[0][2]
+
     def run(self, host_in, host_out) -> None:
-        """Enqueue one host-to-host pass (no synchronisation)."""
+        """Enqueue one host-to-host pass (no synchronisation).  The caller
+        keeps `host_in` unchanged and does not read `host_out` until the
+        pass's copies finished (e.g. `torch.cuda.synchronize()`)."""
         import torch
-        for (a, b), bt in zip(self.groups, self.batches):
+        k = self.turn % len(self.sets)
+        self.turn += 1
+        dev_in, dev_out, batches = self.sets[k]
+        if self.free[k] is not None:
+            self.s_in.wait_event(self.free[k])
+        for (a, b), bt in zip(self.groups, batches):
             lo, hi = int(self.offs[a]), int(self.offs[b])
             e_in = torch.cuda.Event()
             with torch.cuda.stream(self.s_in):
-                self.dev_in[lo:hi].copy_(host_in[lo:hi], non_blocking=True)
+                dev_in[lo:hi].copy_(host_in[lo:hi], non_blocking=True)
                 e_in.record(self.s_in)
             self.s_comp.wait_event(e_in)
             bt.run(graph=True, sync=False)
@@ -389,16 +421,16 @@ class PipelinedBatch:
             e_c.record(self.s_comp)
             self.s_out.wait_event(e_c)
             with torch.cuda.stream(self.s_out):
-                host_out[lo:hi].copy_(self.dev_out[lo:hi], non_blocking=True)
-        # the next pass may overwrite device inputs only after this pass read them
+                host_out[lo:hi].copy_(dev_out[lo:hi], non_blocking=True)
         e_end = torch.cuda.Event()
         e_end.record(self.s_out)
-        self.s_in.wait_event(e_end)
+        self.free[k] = e_end
 
     def close(self):
-        for bt in self.batches:
-            bt.close()
-        self.batches = []
+        for _, _, batches in self.sets:
+            for bt in batches:
+                bt.close()
+        self.sets = []
         self.ctx.close()
 
 

@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--tune", default="cache", choices=["cache", "run", "off"],
                    help="tile configurations: cached autotuner table (tune when absent), retune, or defaults")
     p.add_argument("--e2e-chunks", type=int, default=4, help="pipeline depth of the host-to-host leg")
+    p.add_argument("--e2e-buffers", type=int, default=2,
+                   help="device buffer sets used in turn by consecutive host-to-host steps")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-centerline", action="store_true", help="skip the CenterlineExtraction timing block")
     p.add_argument("--serve-seconds", type=float, default=4.0, help="measured seconds of the serving run")
@@ -316,7 +318,8 @@ def run_bgt(args, rank, world, local):
     # end to end, pipelined: chunks copied in / thinned / copied out on three
     # streams (volumes first: their chains of passes start earliest)
     order = [k for k, it in enumerate(items) if it.ndim == 3] + [k for k, it in enumerate(items) if it.ndim == 2]
-    pb = bgt.PipelinedBatch([items[k].shape for k in order], chunks=args.e2e_chunks, device=local)
+    pb = bgt.PipelinedBatch([items[k].shape for k in order], chunks=args.e2e_chunks, device=local,
+                            buffers=args.e2e_buffers)
     p_in = torch.empty(total, dtype=torch.uint8, pin_memory=True)
     p_out = torch.empty(total, dtype=torch.uint8, pin_memory=True)
     pv = p_in.numpy()
@@ -389,7 +392,8 @@ def run_bgt(args, rank, world, local):
         "e2e": {"value": units_all / (e2e_max * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": total,
                 "d2h_bytes_per_step": total,
                 "path": f"pinned host -> HBM copies, batch C ABI runs, HBM -> pinned host copies; "
-                        f"{args.e2e_chunks} chunks pipelined on three streams (PipelinedBatch)",
+                        f"{args.e2e_chunks} chunks pipelined on three streams, {args.e2e_buffers} device "
+                        f"buffer sets used in turn by consecutive steps (PipelinedBatch)",
                 "serial_value": units / (e2e_serial_ms * 1e-3) / 1e6},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,

@@ -165,3 +165,36 @@ def test_config_shapes_parity(ctx):
     assert np.array_equal(Thinning2D(ves, ctx), po.thin2d(ves)[0])
     vol = synth.trees3d(6, 96, 80, 72, ntrees=3, nell=1)
     assert np.array_equal(Thinning3D(vol, ctx), po.thin3d(vol)[0])
+
+
+@pytest.mark.parametrize("buffers", [1, 2, 3])
+def test_pipelined_batch_host_to_host(buffers):
+    """Consecutive host-to-host passes through PipelinedBatch (chunks on
+    three streams, `buffers` device copies used in turn) give the oracle's
+    output on every pass, also when a pass's inputs change between passes."""
+    import torch
+
+    from begputhinning_b200 import PipelinedBatch
+    rng = np.random.default_rng(40 + buffers)
+    shapes = [(24, 30, 40), (64, 96), (97, 131), (1, 1), (40, 70), (130, 200)]
+    passes = []
+    for p in range(3):
+        items = [blobs3d(rng, *s, 3) if len(s) == 3 else random2d(rng, *s, 0.5) for s in shapes]
+        passes.append(items)
+    pb = PipelinedBatch(shapes, chunks=3, device=0, buffers=buffers)
+    total = pb.total
+    host_in = [torch.empty(total, dtype=torch.uint8, pin_memory=True) for _ in passes]
+    host_out = [torch.zeros(total, dtype=torch.uint8, pin_memory=True) for _ in passes]
+    for hin, items in zip(host_in, passes):
+        v = hin.numpy()
+        for it, o in zip(items, pb.offs):
+            v[o:o + it.size] = it.reshape(-1)
+    for hin, hout in zip(host_in, host_out):
+        pb.run(hin, hout)
+    torch.cuda.synchronize()
+    for hout, items in zip(host_out, passes):
+        v = hout.numpy()
+        for it, o in zip(items, pb.offs):
+            want = po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
+            assert np.array_equal(v[o:o + it.size].reshape(it.shape), want)
+    pb.close()
