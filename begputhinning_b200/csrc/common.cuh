@@ -61,6 +61,7 @@ struct alignas(16) Inst {
     int passes_run;           // passes executed
     int pass_cap;             // safety cap on passes
     int prio;                 // work ring: 0 = critical path (served first), 1 = the rest
+    int gang;                 // 3D: gang arrivals so far (barrier between the gang's passes)
     unsigned long long tiles_run;   // tiles processed (skipped tiles excluded)
     unsigned long long work_words;  // packed core words processed (sum over passes and tiles)
 };

@@ -470,7 +470,8 @@ int bgt::batch_set_input_extent(bgt_batch *b, int id, int inW, int inH, int inD)
 }
 
 // Both rings use `cap` slots; ring r's arrays are seq + r*cap, item + r*cap.
-__global__ void sched_reset_kernel(Sched *S, unsigned *seq, int4 *item, unsigned cap, long long timeout_ns)
+__global__ void sched_reset_kernel(Sched *S, unsigned *seq, int4 *item, unsigned cap, long long timeout_ns,
+                                   int gang_budget)
 {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -486,6 +487,7 @@ __global__ void sched_reset_kernel(Sched *S, unsigned *seq, int4 *item, unsigned
         S->live_prio[1] = 0;
         S->status = 0;
         S->timeout_ns = timeout_ns;
+        S->gang_budget = gang_budget;
     }
     for (unsigned s = i; s < cap; s += gridDim.x * blockDim.x) {
         seq[s] = s;
@@ -537,7 +539,12 @@ static int upload_io(bgt_batch *b)
     b->pack_words = w;
     b->unpack_words = g;
     b->any_out = false;
-    for (int i = 0; i < N; i++) b->any_out |= b->io[i].out != nullptr;
+    b->bytes_only = true;
+    for (int i = 0; i < N; i++) {
+        b->any_out |= b->io[i].out != nullptr;
+        const int dt = io[i].dtype;
+        b->bytes_only &= dtype_size(dt) == 1 && (io[i].mode == 0 || dt == BGT_U8 || dt == BGT_BOOL);
+    }
     cudaError_t e = cudaMemcpyAsync(b->d_io, io.data(), (size_t)N * sizeof(IODesc), cudaMemcpyHostToDevice,
                                     b->ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "I/O table upload");
@@ -563,10 +570,10 @@ static int enqueue_engine(bgt_batch *b, cudaStream_t st, bool capturing)
     const int N = (int)b->items.size();
     stage_event(b->ev[0], st, capturing);
     cudaError_t e = cudaMemsetAsync(b->d_lc, 0x80, b->lc_bytes, st);
-    if (e == cudaSuccess) e = launch_pack_all(b->d_insts, b->d_io, N, b->pack_words, st);
+    if (e == cudaSuccess) e = launch_pack_all(b->d_insts, b->d_io, N, b->pack_words, b->bytes_only, st);
     if (e != cudaSuccess) return cuda_fail(e, "pack");
     sched_reset_kernel<<<std::min<unsigned>(1024, (b->cap + 255) / 256), 256, 0, st>>>(
-        b->d_sched, b->d_seq, b->d_item, b->cap, 20000000000LL);
+        b->d_sched, b->d_seq, b->d_item, b->cap, 20000000000LL, b->grid / 2);
     stage_event(b->ev[1], st, capturing);
     e = launch_engine(b->grid, b->smem, b->d_insts, N, b->d_sched, st);
     if (e != cudaSuccess) return cuda_fail(e, "engine launch");

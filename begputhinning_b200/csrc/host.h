@@ -108,6 +108,7 @@ struct bgt_batch {
     bgt::IODesc *d_io = nullptr;  // per-instance I/O table of the batch-wide pack/unpack
     bool io_dirty = true;
     bool any_out = false;
+    bool bytes_only = false;  // every input one byte wide, tested "byte != 0"
     long long pack_words = 0, unpack_words = 0;
     unsigned cap = 0;
     int smem = 0;

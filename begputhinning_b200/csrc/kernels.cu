@@ -351,11 +351,20 @@ cudaError_t launch_unpack(int dtype, const uint32_t *buf, int W, int H, int D, i
 // index is mapped to its instance by a binary search over io[].wbegin.
 
 // 32 one-byte pixels starting at p -> bit word.  MSB-of-byte gather:
-// bytes that test true become 0x80 after the compare; multiplying the MSB
-// mask by 0x00204081 moves bits 7, 15, 23, 31 to 28..31 without carries.
+// multiplying the MSB mask by 0x00204081 moves bits 7, 15, 23, 31 to 28..31
+// without carries.
 __device__ __forceinline__ uint32_t bytes4_to_bits(uint32_t cmp)
 {
     return ((cmp & 0x80808080u) * 0x00204081u) >> 28;
+}
+
+// 4 bytes -> 4 bits "byte != 0" (bit k for byte k) with integer ALU ops only:
+// the low seven bits of each byte plus 0x7F carry into the byte's MSB
+// exactly when they are nonzero (no carry leaves the byte), and OR-ing the
+// byte back in covers the MSB itself.
+__device__ __forceinline__ uint32_t nz4_to_bits(uint32_t c)
+{
+    return bytes4_to_bits(((c & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | c);
 }
 
 // 32 bytes at word offset Q (0..3) and byte shift sh of 12 loaded words ->
@@ -365,7 +374,7 @@ __device__ __forceinline__ uint32_t pack_from12(const uint32_t (&u)[12], unsigne
 {
     uint32_t w = 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) w |= bytes4_to_bits(__vcmpne4(__funnelshift_r(u[Q + k], u[Q + k + 1], sh), 0u)) << (4 * k);
+    for (int k = 0; k < 8; k++) w |= nz4_to_bits(__funnelshift_r(u[Q + k], u[Q + k + 1], sh)) << (4 * k);
     return w;
 }
 
@@ -398,7 +407,7 @@ __device__ __forceinline__ uint32_t pack_word(const T *p, int n, long long room 
             const uint32_t c[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
             uint32_t w = 0;
 #pragma unroll
-            for (int k = 0; k < 8; k++) w |= bytes4_to_bits(__vcmpne4(c[k], 0u)) << (4 * k);
+            for (int k = 0; k < 8; k++) w |= nz4_to_bits(c[k]) << (4 * k);
             return w;
         }
         // misaligned row: nine aligned words (p-3 .. p+35 at most, all inside
@@ -415,7 +424,7 @@ __device__ __forceinline__ uint32_t pack_word(const T *p, int n, long long room 
             for (int k = 0; k < 8; k++) {
                 const uint32_t next = __ldg(a + k + 1);
                 const uint32_t c = __funnelshift_r(prev, next, s);
-                w |= bytes4_to_bits(__vcmpne4(c, 0u)) << (4 * k);
+                w |= nz4_to_bits(c) << (4 * k);
                 prev = next;
             }
             return w;
@@ -454,6 +463,10 @@ __device__ __forceinline__ int find_io(const IODesc *io, int n, long long g, boo
     return lo;
 }
 
+// BYTES: every instance of the batch has a one-byte input whose test is
+// "byte != 0" (uint8/bool, and int8/char under the 2D rule), so one path
+// serves all and the per-word type dispatch goes away.
+template <bool BYTES>
 __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__restrict__ io, int n,
                                 long long total)
 {
@@ -499,7 +512,9 @@ __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__
             const bool head_ok = off >= 4 || (reinterpret_cast<uintptr_t>(d.in) & 3u) == 0;
             const long long room = head_ok ? (long long)d.inW * d.inH * d.inD - off : 0;
             const long long lead = off;  // one-byte inputs: bytes before this word's first pixel
-            switch (d.dtype) {
+            if constexpr (BYTES) {
+                w = pack_word<uint8_t, 0>((const uint8_t *)d.in + off, cnt, room, lead);
+            } else switch (d.dtype) {
             case BGT_U8: w = pack_word_mode((const uint8_t *)d.in + off, cnt, d.mode, room, lead); break;
             case BGT_I8: w = pack_word_mode((const int8_t *)d.in + off, cnt, d.mode, room, lead); break;
             case BGT_CHAR: w = pack_word_mode((const char *)d.in + off, cnt, d.mode, room, lead); break;
@@ -667,10 +682,13 @@ __global__ void unpack_all_kernel(const Inst *__restrict__ insts, const IODesc *
     }
 }
 
-cudaError_t launch_pack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words,
+cudaError_t launch_pack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words, bool bytes,
                             cudaStream_t st)
 {
-    pack_all_kernel<<<grid_for(total_words, 256), 256, 0, st>>>(d_insts, d_io, n, total_words);
+    if (bytes)
+        pack_all_kernel<true><<<grid_for(total_words, 256), 256, 0, st>>>(d_insts, d_io, n, total_words);
+    else
+        pack_all_kernel<false><<<grid_for(total_words, 256), 256, 0, st>>>(d_insts, d_io, n, total_words);
     return cudaGetLastError();
 }
 
@@ -802,9 +820,10 @@ __device__ __forceinline__ unsigned ld_volatile_u(const unsigned *p)
 }
 
 // Publish n items (instance ii, tiles list[0..n), pass q) on the instance's
-// ring; item.w carries n so a consumer knows the wave size.  The tile threads
-// call it.
-__device__ void produce(Sched *S, int ii, int prio, const int *list, int n, int q)
+// ring; item.w carries n (plus kItemGang for a gang wave) so a consumer
+// knows the wave size.  The tile threads call it.
+constexpr int kItemGang = 1 << 30;
+__device__ void produce(Sched *S, int ii, int prio, const int *list, int n, int q, int gang)
 {
     __shared__ unsigned t0;
     Ring &R = S->ring[prio];
@@ -827,7 +846,7 @@ __device__ void produce(Sched *S, int ii, int prio, const int *list, int n, int 
             atomicOr(&S->status, kErrQueueFull);
             continue;
         }
-        R.item[s] = make_int4(ii, __ldcg(list + i), q, n);
+        R.item[s] = make_int4(ii, __ldcg(list + i), q, n | gang);
         st_rel_u(R.seq + s, t + 1);
     }
     tile_sync();
@@ -893,13 +912,16 @@ __device__ int build_list(Inst &in, int q1, int window, uint32_t *scratch, int s
     return cnt;
 }
 
+// Largest 3D wave that may form a gang.
+constexpr int kGangMaxTiles = 256;
+
 // Build the active list for pass q1 of instance ii and publish it, or retire
 // the instance.  The tile threads call it.  3D instances rebuild the list only at
 // iteration starts (the union pass decides activity for the iteration).
 __device__ void next_wave(Sched *S, Inst *insts, int ii, int q1, int nprev, uint32_t *scratch, int scratch_words)
 {
     Inst &in = insts[ii];
-    __shared__ int cnt;
+    __shared__ int cnt, gang;
     int n;
     if (in.dims == 2) n = build_list(in, q1, in.window, scratch, scratch_words);
     else if (q1 % 6 == 0) n = build_list(in, q1, 6, scratch, scratch_words);
@@ -911,11 +933,23 @@ __device__ void next_wave(Sched *S, Inst *insts, int ii, int q1, int nprev, uint
             atomicOr(&S->status, kErrPassLimit);
             retire = true;
         }
+        gang = 0;
         if (retire) {
             in.converged = n == 0 ? 1 : -1;
         } else {
             in.pass = q1;
             in.done = 0;
+            // a small 3D wave whose list holds for the rest of the iteration
+            // becomes a gang when the budget allows: the CTAs that take its
+            // tiles keep them through the iteration's remaining passes
+            if (in.dims == 3 && q1 % 6 != 5 && n <= kGangMaxTiles) {
+                if (atomicSub(&S->gang_budget, n) >= n) {
+                    in.gang = 0;
+                    gang = kItemGang;
+                } else {
+                    atomicAdd(&S->gang_budget, n);
+                }
+            }
         }
         __threadfence();
         if (retire) {
@@ -926,7 +960,7 @@ __device__ void next_wave(Sched *S, Inst *insts, int ii, int q1, int nprev, uint
     }
     tile_sync();
     const int m = cnt;
-    if (m > 0) produce(S, ii, in.prio, in.list, m, q1);
+    if (m > 0) produce(S, ii, in.prio, in.list, m, q1, gang);
 }
 
 // One CTA per instance: marks reset done by the pack; first wave (pass 0).
@@ -982,10 +1016,26 @@ __device__ __forceinline__ int wait_ticket(Sched *S, int r, unsigned t, int4 &ou
     }
 }
 
+// Wait (bounded by the scheduler's timeout) until *p >= target; acquire.
+__device__ __noinline__ bool wait_at_least(const int *p, int target, const Sched *S)
+{
+    const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
+    for (int spin = 0;; spin++) {
+        if (ld_acquire(p) >= target) return true;
+        if ((spin & 63) == 63 && globaltimer() > t_end) return false;
+        __nanosleep(spin < 16 ? 20 : 100);
+    }
+}
+
 // Persistent engine: thread 0 of each CTA claims a work item (ring 0 first),
 // stages the tile by TMA; the CTA computes it, records its change, counts it
 // against its wave and, for the wave's last tile, builds and publishes the
-// instance's next wave.  Every wait is bounded and reports a status bit.
+// instance's next wave.  The CTAs holding the tiles of a gang wave (a small
+// 3D wave whose tile list stays the same until the iteration ends) instead
+// meet at a per-instance barrier after each pass and go on with the same
+// tile; a budget of half the grid keeps enough CTAs outside gangs to claim
+// every gang's tiles, so no gang waits on a tile nobody can take.  Every
+// wait is bounded and reports a status bit.
 __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched *S, int scratch_words)
 {
     extern __shared__ __align__(128) uint32_t smem_raw[];
@@ -1001,40 +1051,49 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
     }
     __syncthreads();
     uint32_t parity = 0;
+    __shared__ int cont;   // thread 0: the next tile is already staged (gang continuation)
+    __shared__ int gpass;  // thread 0: passes the CTA has run with its gang tile
+    if (threadIdx.x == 0) {
+        cont = 0;
+        gpass = 0;
+    }
     for (;;) {
         if (threadIdx.x == 0) {
-            const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
-            int g = 0;
-            for (int spin = 0;; spin++) {
-                unsigned t;
-                int r = -1;
-                if (take_ticket(S->ring[0], t)) r = 0;
-                else if (take_ticket(S->ring[1], t)) r = 1;
-                if (r >= 0) {
-                    int4 it;
-                    const int w = wait_ticket(S, r, t, it, t_end);
-                    if (w < 0) {
+            int g = cont;
+            if (!cont) {
+                const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
+                for (int spin = 0;; spin++) {
+                    unsigned t;
+                    int r = -1;
+                    if (take_ticket(S->ring[0], t)) r = 0;
+                    else if (take_ticket(S->ring[1], t)) r = 1;
+                    if (r >= 0) {
+                        int4 it;
+                        const int w = wait_ticket(S, r, t, it, t_end);
+                        if (w < 0) {
+                            atomicOr(&S->status, kErrQueueTimeout);
+                            break;
+                        }
+                        if (w == 0) continue;  // abandoned: that ring is finished
+                        item = it;
+                        g = 1;
+                        gpass = 0;
+                        break;
+                    }
+                    if (ld_acquire(&S->live) == 0) break;
+                    if ((spin & 63) == 63 && globaltimer() > t_end) {
                         atomicOr(&S->status, kErrQueueTimeout);
                         break;
                     }
-                    if (w == 0) continue;  // abandoned: that ring is finished
-                    item = it;
-                    g = 1;
-                    issue_tile(insts[it.x], it.z, it.y, smem, &bar);
-                    break;
+                    __nanosleep(spin < 32 ? 20 : 200);
                 }
-                if (ld_acquire(&S->live) == 0) break;
-                if ((spin & 63) == 63 && globaltimer() > t_end) {
-                    atomicOr(&S->status, kErrQueueTimeout);
-                    break;
-                }
-                __nanosleep(spin < 32 ? 20 : 200);
             }
+            if (g) issue_tile(insts[item.x], item.z, item.y, smem, &bar);
             got = g;
         }
         __syncthreads();
         if (!got) break;
-        const int ii = item.x, tile = item.y, q = item.z, nwave = item.w;
+        const int ii = item.x, tile = item.y, q = item.z, nwave = item.w & ~kItemGang;
         Inst &in = insts[ii];
         if (!mbar_wait_bounded(&bar, parity)) {
             if (threadIdx.x == 0) atomicOr(&S->status, kErrTmaTimeout);
@@ -1047,10 +1106,29 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
                 if (in.dims == 2) in.act[tile] = (uint8_t)(m & kAllBands);  // bands the next wave reads
             }
             __threadfence();
-            const int d = atomicAdd(&in.done, 1);
-            last = d == nwave - 1;
-            atomicAdd(&in.tiles_run, 1ull);
-            atomicAdd(&in.work_words, (unsigned long long)tile_core_words(in, tile));
+            cont = 0;
+            last = 0;
+            const bool in_gang = (item.w & kItemGang) != 0;
+            if (in_gang && q % 6 != 5) {
+                // gang: once every member has finished pass q, take the same
+                // tile in pass q + 1 without going through the ring
+                atomicAdd(&in.gang, 1);
+                atomicAdd(&in.tiles_run, 1ull);
+                atomicAdd(&in.work_words, (unsigned long long)tile_core_words(in, tile));
+                gpass += 1;
+                if (wait_at_least(&in.gang, nwave * gpass, S)) {
+                    item.z = q + 1;  // staged at the top of the loop
+                    cont = 1;
+                } else {
+                    atomicOr(&S->status, kErrQueueTimeout);
+                }
+            } else {
+                const int d = atomicAdd(&in.done, 1);
+                last = d == nwave - 1;
+                if (last && in_gang) atomicAdd(&S->gang_budget, nwave);  // the gang dissolves
+                atomicAdd(&in.tiles_run, 1ull);
+                atomicAdd(&in.work_words, (unsigned long long)tile_core_words(in, tile));
+            }
         }
         __syncthreads();
         if (last) {

@@ -41,6 +41,7 @@ struct Sched {
     Ring ring[2];       // 0: critical-path instances, 1: the rest
     int live;           // instances not yet converged
     int live_prio[2];   // ... per ring (a ring with no live instance gets no more items)
+    int gang_budget;    // CTAs that may still join gangs (the rest keep claiming)
     int status;         // error bits
     long long timeout_ns;
 };
@@ -86,7 +87,8 @@ struct alignas(16) IODesc {
 };
 
 // Launchers (stream-ordered, no host synchronisation).
-cudaError_t launch_pack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words,
+// bytes: every input is one byte wide and tested "byte != 0" (see pack_all_kernel)
+cudaError_t launch_pack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words, bool bytes,
                             cudaStream_t st);
 cudaError_t launch_unpack_all(const Inst *d_insts, const IODesc *d_io, int n, long long total_words,
                               cudaStream_t st);

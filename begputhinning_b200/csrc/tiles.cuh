@@ -40,30 +40,41 @@ __host__ __device__ constexpr int band_bit(int dy, int dx)
 }
 
 // ---------------------------------------------------------------- 2D ------
-// One subiteration on the lane's S+2 words.  Word steps whose centre words
-// are empty in every lane of the warp are skipped (nothing to delete there).
+// The rule on one word of the lane's row: `o` the word, `n`/`p` the words
+// after/before it (pass-start values).  Returns the word after deletion.
+template <int DIR>
+__device__ __forceinline__ uint32_t word2d(uint32_t o, uint32_t n, uint32_t p)
+{
+    const uint32_t xp = at_xp1(o, n), xm = at_xm1(o, p);
+    uint32_t X[8];
+    X[0] = __shfl_up_sync(kFull, o, 1);
+    X[1] = __shfl_up_sync(kFull, xp, 1);
+    X[7] = __shfl_up_sync(kFull, xm, 1);
+    X[4] = __shfl_down_sync(kFull, o, 1);
+    X[3] = __shfl_down_sync(kFull, xp, 1);
+    X[5] = __shfl_down_sync(kFull, xm, 1);
+    X[2] = xp;
+    X[6] = xm;
+    return o & ~rule2d<DIR>(X);
+}
+
+// One subiteration on the lane's S+2 words, two words per step so that the
+// shuffles and rules of both overlap.  Steps whose two centre words are empty
+// in every lane of the warp are skipped (nothing to delete there).
 template <int S, int DIR>
 __device__ __forceinline__ void subit2d(uint32_t (&v)[S + 2])
 {
+    static_assert(S % 2 == 0, "pairs of words");
     uint32_t prev_old = 0;
 #pragma unroll
-    for (int j = 0; j < S + 2; j++) {
-        const uint32_t old_j = v[j];
-        if (__any_sync(kFull, old_j != 0u)) {
-            const uint32_t old_n = j + 1 < S + 2 ? v[j + 1] : 0u;
-            const uint32_t xp = at_xp1(old_j, old_n), xm = at_xm1(old_j, prev_old);
-            uint32_t X[8];
-            X[0] = __shfl_up_sync(kFull, old_j, 1);
-            X[1] = __shfl_up_sync(kFull, xp, 1);
-            X[7] = __shfl_up_sync(kFull, xm, 1);
-            X[4] = __shfl_down_sync(kFull, old_j, 1);
-            X[3] = __shfl_down_sync(kFull, xp, 1);
-            X[5] = __shfl_down_sync(kFull, xm, 1);
-            X[2] = xp;
-            X[6] = xm;
-            v[j] = old_j & ~rule2d<DIR>(X);
+    for (int j = 0; j < S + 2; j += 2) {
+        const uint32_t o0 = v[j], o1 = v[j + 1];
+        const uint32_t on = j + 2 < S + 2 ? v[j + 2] : 0u;
+        if (__any_sync(kFull, (o0 | o1) != 0u)) {
+            v[j] = word2d<DIR>(o0, o1, prev_old);
+            v[j + 1] = word2d<DIR>(o1, on, o0);
         }
-        prev_old = old_j;
+        prev_old = o1;
     }
 }
 
