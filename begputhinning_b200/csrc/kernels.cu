@@ -439,6 +439,38 @@ __device__ __forceinline__ uint32_t pack_word(const T *p, int n, long long room 
     return w;
 }
 
+// 32 one-byte pixels from p (n < 32 at a row's ragged end) -> "byte != 0"
+// bits, without branches that depend on p's alignment: three aligned 16-byte
+// loads cover p .. p+31 (they may run past the row into the next one, never
+// past the input: `room` and `lead` as in pack_word), the 12 loaded words are
+// shifted by p's word offset in two conditional-select stages and by its byte
+// offset with funnel shifts, and bits at and past n are cleared.  Words too
+// close to either end of the input take the byte loop.
+__device__ __forceinline__ uint32_t pack_bytes32(const uint8_t *p, int n, long long room, long long lead)
+{
+    const uintptr_t pa = reinterpret_cast<uintptr_t>(p);
+    const unsigned o = (unsigned)(pa & 15u);
+    if ((long long)o <= lead && (long long)(48u - o) <= room) {
+        const uint4 *a16 = reinterpret_cast<const uint4 *>(pa & ~uintptr_t(15));
+        const uint4 A = __ldg(a16), B = __ldg(a16 + 1), C = __ldg(a16 + 2);
+        const uint32_t u[12] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w, C.x, C.y, C.z, C.w};
+        const bool s2 = (o & 8u) != 0, s1 = (o & 4u) != 0;
+        uint32_t t[10], v[9];
+#pragma unroll
+        for (int i = 0; i < 10; i++) t[i] = s2 ? u[i + 2] : u[i];
+#pragma unroll
+        for (int i = 0; i < 9; i++) v[i] = s1 ? t[i + 1] : t[i];
+        const unsigned sh = (o & 3u) * 8u;
+        uint32_t w = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) w |= nz4_to_bits(__funnelshift_r(v[k], v[k + 1], sh)) << (4 * k);
+        return n >= 32 ? w : w & ((1u << n) - 1u);
+    }
+    uint32_t w = 0;
+    for (int b = 0; b < n; b++) w |= (uint32_t)(p[b] != 0) << b;
+    return w;
+}
+
 template <typename T>
 __device__ __forceinline__ uint32_t pack_word_mode(const T *p, int n, int mode, long long room, long long lead = 0)
 {
@@ -513,7 +545,7 @@ __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__
             const long long room = head_ok ? (long long)d.inW * d.inH * d.inD - off : 0;
             const long long lead = off;  // one-byte inputs: bytes before this word's first pixel
             if constexpr (BYTES) {
-                w = pack_word<uint8_t, 0>((const uint8_t *)d.in + off, cnt, room, lead);
+                w = pack_bytes32((const uint8_t *)d.in + off, cnt, room, lead);
             } else switch (d.dtype) {
             case BGT_U8: w = pack_word_mode((const uint8_t *)d.in + off, cnt, d.mode, room, lead); break;
             case BGT_I8: w = pack_word_mode((const int8_t *)d.in + off, cnt, d.mode, room, lead); break;
