@@ -527,10 +527,10 @@ static int upload_io(bgt_batch *b)
         io[i].dTZ = make_fastdiv((uint32_t)std::max(1, in.TZ));
         w += (long long)in.P * in.H * in.D;
         if (dtype_size(s.dtype) == 1 && s.out) {
-            // unpack unit: 16-byte-aligned chunk of the output
+            // unpack unit: 32-byte-aligned chunk of the output
             const uintptr_t o = reinterpret_cast<uintptr_t>(s.out);
             const uintptr_t end = o + (uintptr_t)in.W * in.H * in.D;
-            g += (long long)((end - (o & ~uintptr_t(15)) + 15) / 16);
+            g += (long long)((end - (o & ~uintptr_t(31)) + 31) / 32);
         } else {
             // unpack unit: packed word (rows x ceil(W/32))
             g += (long long)((in.W + 31) / 32) * in.H * in.D;

@@ -663,6 +663,52 @@ __device__ __forceinline__ void unpack_chunk16(const uint32_t *buf, int W, int P
     }
 }
 
+// 32 consecutive bits of a packed row starting at pixel x; the word after
+// x's word is read only when x is not word-aligned, and the caller
+// guarantees it lies inside the packed buffer.
+__device__ __forceinline__ uint32_t row_bits32(const uint32_t *r, int x)
+{
+    const uint32_t w0 = __ldg(r + (x >> 5));
+    const uint32_t w1 = (x & 31) ? __ldg(r + (x >> 5) + 1) : 0u;
+    return __funnelshift_r(w0, w1, x & 31);
+}
+
+// One-byte outputs, unit = one 32-byte-aligned chunk of the output: two
+// 128-bit stores when the chunk lies inside the output and the image is at
+// least 32 pixels wide (the chunk then spans at most two rows); otherwise
+// its two 16-byte halves go through unpack_chunk16.
+__device__ __forceinline__ void unpack_chunk32(const uint32_t *buf, int W, int P, long long n, const IODesc &d,
+                                               long long c)
+{
+    const uintptr_t out = reinterpret_cast<uintptr_t>(d.out);
+    const uintptr_t a = (out & ~uintptr_t(31)) + (uintptr_t)c * 32u;
+    if (a >= out && (long long)(a + 32 - out) <= n && W >= 32) {
+        const uint32_t lo = (uint32_t)(a - out);
+        const uint32_t row = fdiv(d.dW, lo);
+        const int x = (int)(lo - row * (uint32_t)W);
+        const uint32_t *r = buf + (size_t)row * P;
+        uint32_t bits;
+        if (x + 32 <= W) {
+            bits = row_bits32(r, x);
+        } else {  // the chunk runs into the next row
+            const int n0 = W - x;
+            bits = (row_bits32(r, x) & ((1u << n0) - 1u)) | (__ldg(r + P) << n0);
+        }
+        uint4 *o = reinterpret_cast<uint4 *>(a);
+        o[0] = make_uint4(bits4_to_bytes(bits & 15u), bits4_to_bytes((bits >> 4) & 15u),
+                          bits4_to_bytes((bits >> 8) & 15u), bits4_to_bytes((bits >> 12) & 15u));
+        o[1] = make_uint4(bits4_to_bytes((bits >> 16) & 15u), bits4_to_bytes((bits >> 20) & 15u),
+                          bits4_to_bytes((bits >> 24) & 15u), bits4_to_bytes(bits >> 28));
+        return;
+    }
+    const uintptr_t base16 = out & ~uintptr_t(15);
+    for (int h = 0; h < 2; h++) {
+        const uintptr_t ah = a + 16u * (uintptr_t)h;
+        if (ah + 16 <= out || (ah >= out && (long long)(ah - out) >= n)) continue;  // outside the output
+        unpack_chunk16(buf, W, P, n, d, (long long)((ah - base16) / 16u));
+    }
+}
+
 __global__ void unpack_all_kernel(const Inst *__restrict__ insts, const IODesc *__restrict__ io, int n,
                                   long long total)
 {
@@ -693,7 +739,7 @@ __global__ void unpack_all_kernel(const Inst *__restrict__ insts, const IODesc *
         }
         if (!d.out) continue;
         if (bytes1) {
-            unpack_chunk16(buf, W, P, npx, d, g - kb);
+            unpack_chunk32(buf, W, P, npx, d, g - kb);
             continue;
         }
         const uint32_t i = (uint32_t)(g - kb);
@@ -1014,19 +1060,10 @@ __global__ void __launch_bounds__(kThreads) engine_seed_kernel(Inst *insts, int 
     }
 }
 
-// Take a ticket of ring R (one fetch-and-add, no retry loop) when the ring
-// looks non-empty.  Several CTAs may see the same last item, so a ticket can
-// run past the items produced so far; its holder then waits for the ring's
-// next item (see wait_ticket).
-__device__ __forceinline__ bool take_ticket(Ring &R, unsigned &t)
-{
-    const unsigned h = ld_volatile_u(&R.head);
-    const unsigned tl = ld_volatile_u(&R.tail);
-    if ((int)(tl - h) <= 0) return false;
-    t = atomicAdd(&R.head, 1u);
-    return true;
-}
-
+// A consumer takes a ticket of a ring (one fetch-and-add, no retry loop)
+// when the ring looks non-empty.  Several CTAs may see the same last item, so
+// a ticket can run past the items produced so far; its holder then waits for
+// the ring's next item (see wait_ticket).
 // Wait for the item of ticket t of ring r.  Returns 1 with the item, 0 when
 // the ticket can never be filled (every instance of that ring retired and t
 // is past the final tail: the ticket is abandoned), -1 on timeout.
@@ -1097,8 +1134,16 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
                 for (int spin = 0;; spin++) {
                     unsigned t;
                     int r = -1;
-                    if (take_ticket(S->ring[0], t)) r = 0;
-                    else if (take_ticket(S->ring[1], t)) r = 1;
+                    // both rings' counters in one round trip; ring 0 first
+                    const unsigned h0 = ld_volatile_u(&S->ring[0].head), t0 = ld_volatile_u(&S->ring[0].tail);
+                    const unsigned h1 = ld_volatile_u(&S->ring[1].head), t1 = ld_volatile_u(&S->ring[1].tail);
+                    if ((int)(t0 - h0) > 0) {
+                        t = atomicAdd(&S->ring[0].head, 1u);
+                        r = 0;
+                    } else if ((int)(t1 - h1) > 0) {
+                        t = atomicAdd(&S->ring[1].head, 1u);
+                        r = 1;
+                    }
                     if (r >= 0) {
                         int4 it;
                         const int w = wait_ticket(S, r, t, it, t_end);
