@@ -270,6 +270,11 @@ class Batch:
         self.shapes.append(tuple(shape))
         return i.value
 
+    def set_grid(self, ctas: int) -> None:
+        """Cap the persistent engine's grid at `ctas` CTAs (0: no cap);
+        call before finalize()."""
+        check(lib().bgt_batch_set_grid(self.h, ctas))
+
     def finalize(self) -> None:
         check(lib().bgt_batch_finalize(self.h))
 

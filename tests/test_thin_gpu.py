@@ -198,3 +198,32 @@ def test_pipelined_batch_host_to_host(buffers):
             want = po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
             assert np.array_equal(v[o:o + it.size].reshape(it.shape), want)
     pb.close()
+
+
+@pytest.mark.parametrize("ctas", [1, 2, 3, 8, 64])
+def test_engine_small_grids_and_gangs(ctx, ctas):
+    """Volumes and images in one batch on a capped engine grid: with few CTAs
+    the gang budget (half the grid) admits only the smallest 3D waves, or
+    none, so gangs, ordinary waves and gang-less volumes run side by side;
+    every instance must converge to the oracle's result."""
+    import torch
+
+    from begputhinning_b200 import Batch
+    rng = np.random.default_rng(70 + ctas)
+    items = [blobs3d(rng, 20 + 7 * k, 33, 40 + 5 * k, 3) for k in range(4)]
+    items += [random3d(rng, 9, 12, 10, 0.5), blobs2d(rng, 97, 131, 10), random2d(rng, 64, 96, 0.5)]
+    b = Batch(ctx)
+    ids = [b.add(it.shape) for it in items]
+    b.set_grid(ctas)
+    b.finalize()
+    ins = [torch.from_numpy(it).cuda() for it in items]
+    outs = [torch.empty_like(t) for t in ins]
+    for i, t, o in zip(ids, ins, outs):
+        b.set_io(i, t, o)
+    for rep in range(2):
+        b.run()
+        for k, (it, o) in enumerate(zip(items, outs)):
+            want = po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
+            assert np.array_equal(o.cpu().numpy(), want), f"instance {k}, run {rep}"
+            assert b.stats(ids[k])["converged"] == 1
+    b.close()
