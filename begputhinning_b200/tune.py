@@ -116,15 +116,16 @@ def save_cache(table: dict, device: int = 0, path: str = CACHE) -> None:
         json.dump(data, f, indent=1, sort_keys=True)
 
 
-def load_cache(device: int = 0, path: str = CACHE) -> dict:
-    """Apply the cached table of this GPU (if any); returns it."""
+def load_cache(device: int = 0, path: str = CACHE):
+    """Apply the cached table of this GPU and return it; None when this GPU
+    has no entry.  An empty entry means the tuner kept every default."""
     if not os.path.exists(path):
-        return {}
+        return None
     with open(path) as f:
         data = json.load(f)
     entry = data.get(gpu_name(device))
-    if not entry:
-        return {}
+    if entry is None:
+        return None
     table = {(int(k.split(":")[0]), int(k.split(":")[1])): v for k, v in entry.items()}
     apply(table)
     return table

@@ -205,13 +205,14 @@ def run_bgt(args, rank, world, local):
     dev = torch.device("cuda", local)
     items = workload(args.seed + 1000 * rank, args.n2d, args.n3d)
     from begputhinning_b200 import tune
-    table = {}
+    table = None
     if args.tune == "cache":
         table = tune.load_cache(local)
-    if args.tune == "run" or (args.tune == "cache" and not table):
+    if args.tune == "run" or (args.tune == "cache" and table is None):
         table = tune.autotune(items, device=local)["table"]
         if rank == 0:
             tune.save_cache(table, local)
+    table = table or {}
     sizes = [it.size for it in items]
     units = int(sum(sizes))
     total = sum(sizes)
