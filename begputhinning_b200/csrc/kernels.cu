@@ -1122,9 +1122,13 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
     uint32_t parity = 0;
     __shared__ int cont;   // thread 0: the next tile is already staged (gang continuation)
     __shared__ int gpass;  // thread 0: passes the CTA has run with its gang tile
+    __shared__ int pend;   // thread 0: a second bulk-ring ticket is held
+    __shared__ unsigned pend_t;
     if (threadIdx.x == 0) {
         cont = 0;
         gpass = 0;
+        pend = 0;
+        pend_t = 0;
     }
     for (;;) {
         if (threadIdx.x == 0) {
@@ -1132,17 +1136,35 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
             if (!cont) {
                 const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
                 for (int spin = 0;; spin++) {
-                    unsigned t;
+                    unsigned t = 0;
                     int r = -1;
-                    // both rings' counters in one round trip; ring 0 first
-                    const unsigned h0 = ld_volatile_u(&S->ring[0].head), t0 = ld_volatile_u(&S->ring[0].tail);
-                    const unsigned h1 = ld_volatile_u(&S->ring[1].head), t1 = ld_volatile_u(&S->ring[1].tail);
-                    if ((int)(t0 - h0) > 0) {
+                    const bool ring0_waiting =
+                        pend && (int)(ld_volatile_u(&S->ring[0].tail) - ld_volatile_u(&S->ring[0].head)) > 0;
+                    if (pend && !ring0_waiting) {  // second ticket of the last double claim
+                        r = 1;
+                        t = pend_t;
+                        pend = 0;
+                    } else if (ring0_waiting) {  // ring 0 first; the held ticket waits
                         t = atomicAdd(&S->ring[0].head, 1u);
                         r = 0;
-                    } else if ((int)(t1 - h1) > 0) {
-                        t = atomicAdd(&S->ring[1].head, 1u);
-                        r = 1;
+                    } else {
+                        // both rings' counters in one round trip; ring 0 first
+                        const unsigned h0 = ld_volatile_u(&S->ring[0].head), t0 = ld_volatile_u(&S->ring[0].tail);
+                        const unsigned h1 = ld_volatile_u(&S->ring[1].head), t1 = ld_volatile_u(&S->ring[1].tail);
+                        if ((int)(t0 - h0) > 0) {
+                            t = atomicAdd(&S->ring[0].head, 1u);
+                            r = 0;
+                        } else if ((int)(t1 - h1) >= 2 * (int)gridDim.x) {
+                            // deep bulk ring: two tickets for one fetch-and-add; the
+                            // second is waited for only after the first tile is done
+                            t = atomicAdd(&S->ring[1].head, 2u);
+                            r = 1;
+                            pend = 1;
+                            pend_t = t + 1;
+                        } else if ((int)(t1 - h1) > 0) {
+                            t = atomicAdd(&S->ring[1].head, 1u);
+                            r = 1;
+                        }
                     }
                     if (r >= 0) {
                         int4 it;
