@@ -1096,6 +1096,9 @@ __device__ __noinline__ bool wait_at_least(const int *p, int target, const Sched
     }
 }
 
+// Most bulk-ring tickets one CTA takes with one fetch-and-add.
+constexpr int kMaxClaim = 4;
+
 // Persistent engine: thread 0 of each CTA claims a work item (ring 0 first),
 // stages the tile by TMA; the CTA computes it, records its change, counts it
 // against its wave and, for the wave's last tile, builds and publishes the
@@ -1122,7 +1125,7 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
     uint32_t parity = 0;
     __shared__ int cont;   // thread 0: the next tile is already staged (gang continuation)
     __shared__ int gpass;  // thread 0: passes the CTA has run with its gang tile
-    __shared__ int pend;   // thread 0: a second bulk-ring ticket is held
+    __shared__ int pend;   // thread 0: bulk-ring tickets still held (pend_t, pend_t + 1, ...)
     __shared__ unsigned pend_t;
     if (threadIdx.x == 0) {
         cont = 0;
@@ -1140,10 +1143,11 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
                     int r = -1;
                     const bool ring0_waiting =
                         pend && (int)(ld_volatile_u(&S->ring[0].tail) - ld_volatile_u(&S->ring[0].head)) > 0;
-                    if (pend && !ring0_waiting) {  // second ticket of the last double claim
+                    if (pend && !ring0_waiting) {  // next held ticket of the last multiple claim
                         r = 1;
                         t = pend_t;
-                        pend = 0;
+                        pend -= 1;
+                        pend_t = t + 1;
                     } else if (ring0_waiting) {  // ring 0 first; the held ticket waits
                         t = atomicAdd(&S->ring[0].head, 1u);
                         r = 0;
@@ -1155,11 +1159,14 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
                             t = atomicAdd(&S->ring[0].head, 1u);
                             r = 0;
                         } else if ((int)(t1 - h1) >= 2 * (int)gridDim.x) {
-                            // deep bulk ring: two tickets for one fetch-and-add; the
-                            // second is waited for only after the first tile is done
-                            t = atomicAdd(&S->ring[1].head, 2u);
+                            // deep bulk ring: k consecutive tickets for one
+                            // fetch-and-add (k = items per CTA in the ring, at most
+                            // kMaxClaim); each held ticket is waited for only after
+                            // the tile before it is done
+                            const int k = min(kMaxClaim, (int)(t1 - h1) / (int)gridDim.x);
+                            t = atomicAdd(&S->ring[1].head, (unsigned)k);
                             r = 1;
-                            pend = 1;
+                            pend = k - 1;
                             pend_t = t + 1;
                         } else if ((int)(t1 - h1) > 0) {
                             t = atomicAdd(&S->ring[1].head, 1u);
