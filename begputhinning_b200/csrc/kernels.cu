@@ -1096,6 +1096,26 @@ __device__ __noinline__ bool wait_at_least(const int *p, int target, const Sched
     }
 }
 
+// One look at ticket t of ring r (no waiting): 1 with the item (the slot is
+// released as by wait_ticket), 0 when it is not filled yet.
+__device__ __forceinline__ int poll_ticket(Sched *S, int r, unsigned t, int4 &out)
+{
+    Ring &R = S->ring[r];
+    const unsigned s = t % R.cap;
+    if (ld_acq_u(R.seq + s) != t + 1) return 0;
+    out = __ldcg(R.item + s);
+    st_rel_u(R.seq + s, t + R.cap);
+    return 1;
+}
+
+// Shared-memory scratch of the engine's next-wave builder, behind the tile
+// box: the next tile's box may be in flight while a wave is built.
+constexpr int kEngineScratchWords = 1024;
+static int engine_smem_bytes(int box_bytes)
+{
+    return 128 + (box_bytes + 127) / 128 * 128 + kEngineScratchWords * 4;
+}
+
 // Most bulk-ring tickets one CTA takes with one fetch-and-add.
 constexpr int kMaxClaim = 4;
 
@@ -1108,16 +1128,18 @@ constexpr int kMaxClaim = 4;
 // tile; a budget of half the grid keeps enough CTAs outside gangs to claim
 // every gang's tiles, so no gang waits on a tile nobody can take.  Every
 // wait is bounded and reports a status bit.
-__global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched *S, int scratch_words)
+__global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched *S, int box_words)
 {
     extern __shared__ __align__(128) uint32_t smem_raw[];
     uint32_t *smem = align128(smem_raw);
+    uint32_t *scratch = smem + (box_words + 31) / 32 * 32;
     __shared__ __align__(8) uint64_t bar;
-    __shared__ int4 item;
-    __shared__ int got, last;
+    __shared__ int4 item, nitem;
+    __shared__ int got, last, ngot;
     __shared__ uint32_t band;
     if (threadIdx.x == 0) {
         band = 0;
+        ngot = 0;
         mbar_init(&bar, 1);
         fence_mbar_init();
     }
@@ -1136,7 +1158,14 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
     for (;;) {
         if (threadIdx.x == 0) {
             int g = cont;
-            if (!cont) {
+            bool staged = false;
+            if (!cont && ngot) {  // a held ticket's tile, staged by thread 32 during the bookkeeping
+                item = nitem;
+                ngot = 0;
+                g = 1;
+                gpass = 0;
+                staged = true;
+            } else if (!cont) {
                 const unsigned long long t_end = globaltimer() + (unsigned long long)S->timeout_ns;
                 for (int spin = 0;; spin++) {
                     unsigned t = 0;
@@ -1194,18 +1223,32 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
                     __nanosleep(spin < 32 ? 20 : 200);
                 }
             }
-            if (g) issue_tile(insts[item.x], item.z, item.y, smem, &bar);
+            if (g && !staged) issue_tile(insts[item.x], item.z, item.y, smem, &bar);
             got = g;
         }
         __syncthreads();
         if (!got) break;
         const int ii = item.x, tile = item.y, q = item.z, nwave = item.w & ~kItemGang;
+        const bool gang_tile = (item.w & kItemGang) != 0;
         Inst &in = insts[ii];
         if (!mbar_wait_bounded(&bar, parity)) {
             if (threadIdx.x == 0) atomicOr(&S->status, kErrTmaTimeout);
         }
         parity ^= 1u;
         const uint32_t m = run_tile(in, q, tile, smem, &band);  // ends with a barrier: smem is free again
+        if (threadIdx.x == 32 && pend > 0 && !(gang_tile && q % 6 != 5) &&
+            (int)(ld_volatile_u(&S->ring[0].tail) - ld_volatile_u(&S->ring[0].head)) <= 0) {
+            // while thread 0 records this tile, stage the next held ticket's
+            // tile if its item is already there (one look, no waiting)
+            int4 it;
+            if (poll_ticket(S, 1, pend_t, it)) {
+                pend -= 1;
+                pend_t += 1;
+                nitem = it;
+                ngot = 1;
+                issue_tile(insts[it.x], it.z, it.y, smem, &bar);
+            }
+        }
         if (threadIdx.x == 0) {
             if (m & kTileChanged) {
                 in.lc[tile] = q;
@@ -1214,8 +1257,7 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
             __threadfence();
             cont = 0;
             last = 0;
-            const bool in_gang = (item.w & kItemGang) != 0;
-            if (in_gang && q % 6 != 5) {
+            if (gang_tile && q % 6 != 5) {
                 // gang: once every member has finished pass q, take the same
                 // tile in pass q + 1 without going through the ring
                 atomicAdd(&in.gang, 1);
@@ -1231,7 +1273,7 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
             } else {
                 const int d = atomicAdd(&in.done, 1);
                 last = d == nwave - 1;
-                if (last && in_gang) atomicAdd(&S->gang_budget, nwave);  // the gang dissolves
+                if (last && gang_tile) atomicAdd(&S->gang_budget, nwave);  // the gang dissolves
                 atomicAdd(&in.tiles_run, 1ull);
                 atomicAdd(&in.work_words, (unsigned long long)tile_core_words(in, tile));
             }
@@ -1239,7 +1281,7 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
         __syncthreads();
         if (last) {
             __threadfence();
-            next_wave(S, insts, ii, q + 1, nwave, smem, scratch_words);
+            next_wave(S, insts, ii, q + 1, nwave, scratch, kEngineScratchWords);
         }
         __syncthreads();
     }
@@ -1248,13 +1290,14 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
 int engine_max_blocks_per_sm(int smem)
 {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel, kThreads, smem + 128);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, engine_kernel, kThreads, engine_smem_bytes(smem));
     return n;
 }
 
 cudaError_t engine_set_smem(int smem)
 {
-    cudaError_t e = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem + 128);
+    cudaError_t e = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         engine_smem_bytes(smem));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(plain_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem + 128);
 }
@@ -1264,7 +1307,7 @@ cudaError_t launch_engine(int grid, int smem, Inst *d_insts, int ninst, Sched *d
     engine_seed_kernel<<<std::min(ninst, 148 * 8), kThreads, 0, st>>>(d_insts, ninst, d_sched);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    engine_kernel<<<grid, kThreads, smem + 128, st>>>(d_insts, d_sched, smem / 4);
+    engine_kernel<<<grid, kThreads, engine_smem_bytes(smem), st>>>(d_insts, d_sched, smem / 4);
     return cudaGetLastError();
 }
 
