@@ -78,12 +78,32 @@ __device__ __forceinline__ void subit2d(uint32_t (&v)[S + 2])
     }
 }
 
+// The pass's last subiteration: only the S core words are kept afterwards,
+// so they are processed as the pairs (1,2) .. (S-1,S) and the two halo
+// words are left as they are.
+template <int S, int DIR>
+__device__ __forceinline__ void subit2d_core(uint32_t (&v)[S + 2])
+{
+    uint32_t prev_old = v[0];
+#pragma unroll
+    for (int j = 1; j <= S; j += 2) {
+        const uint32_t o0 = v[j], o1 = v[j + 1], on = v[j + 2];
+        if (__any_sync(kFull, (o0 | o1) != 0u)) {
+            v[j] = word2d<DIR>(o0, o1, prev_old);
+            v[j + 1] = word2d<DIR>(o1, on, o0);
+        }
+        prev_old = o1;
+    }
+}
+
 template <int K, int S, int PH, int I = 0>
 __device__ __forceinline__ void run_subits2d(uint32_t (&v)[S + 2])
 {
-    if constexpr (I < K) {
+    if constexpr (I + 1 < K) {
         subit2d<S, (PH + I) & 3>(v);
         run_subits2d<K, S, PH, I + 1>(v);
+    } else if constexpr (I + 1 == K) {
+        subit2d_core<S, (PH + I) & 3>(v);
     }
 }
 
