@@ -406,7 +406,10 @@ __device__ uint32_t tile3d(const Inst &in, int q, int tile, const uint32_t *smem
         const bool live = lane_live && z < in.D;
         const uint32_t val = B[4];
         uint32_t nv = val;
-        if (__any_sync(kFull, live && val != 0u)) {
+        // passes 1..5 delete only voxels of the iteration's union: words whose
+        // union is empty in every lane skip the rule
+        const uint32_t cand = MODE == 0 ? val : val & usm[(zz * BH + lane) * NWX + warp];
+        if (__any_sync(kFull, live && cand != 0u)) {
             uint32_t g[27];
 #pragma unroll
             for (int i = 0; i < 9; i++) {
@@ -422,8 +425,7 @@ __device__ uint32_t tile3d(const Inst &in, int q, int tile, const uint32_t *smem
                 if (live) in.uni[idx] = un & val;
                 del = val & du;
             } else {
-                const uint32_t un = usm[(zz * BH + lane) * NWX + warp];
-                del = val & rule3d<MODE>(g) & un;
+                del = cand & rule3d<MODE>(g);
             }
             nv = val & ~del;
             if (live) chg |= del;
