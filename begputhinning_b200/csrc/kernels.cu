@@ -1147,7 +1147,11 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
     uint32_t parity = 0;
     __shared__ int cont;   // thread 0: the next tile is already staged (gang continuation)
     __shared__ int gpass;  // thread 0: passes the CTA has run with its gang tile
-    __shared__ int pend;   // thread 0: bulk-ring tickets still held (pend_t, pend_t + 1, ...)
+    // Bulk-ring tickets still held (pend_t, pend_t + 1, ...).  Thread 0 owns
+    // them, except between run_tile and the next barrier, when thread 32 may
+    // take the first one (and stage its tile, setting ngot/nitem) while
+    // thread 0, busy recording the tile, does not touch them.
+    __shared__ int pend;
     __shared__ unsigned pend_t;
     if (threadIdx.x == 0) {
         cont = 0;
