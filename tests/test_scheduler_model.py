@@ -214,12 +214,14 @@ class CTA:
         return True
 
 
-def run_model(seed, grid, n2d, n3d, eager_claim=False):
+def run_model(seed, grid, n2d, n3d, eager_claim=False, budget=None):
     rng = random.Random(seed)
     insts = [Inst(rng, 2) for _ in range(n2d)] + [Inst(rng, 3) for _ in range(n3d)]
     rng.shuffle(insts)
     m = Model(rng, insts, grid)
     m.eager_claim = eager_claim
+    if budget is not None:
+        m.budget = m.budget0 = budget
     for ii, inst in enumerate(insts):  # the seed kernel
         m.live += 1
         m.live_prio[inst.prio] += 1
@@ -259,6 +261,14 @@ def test_schedule_model_many_volumes_small_grid():
     # more gang-eligible volumes than CTAs: the budget must keep claimers free
     for seed in range(20):
         run_model(1000 + seed, grid=4, n2d=1, n3d=8)
+
+
+@pytest.mark.parametrize("grid", [2, 4, 6])
+def test_schedule_model_any_budget_up_to_the_grid(grid):
+    # the engine reserves half the grid; the argument holds for any budget up
+    # to the grid (all live gangs together fit on the CTAs at once)
+    for seed in range(15):
+        run_model(3000 + 7 * seed + grid, grid=grid, n2d=2, n3d=6, budget=grid)
 
 
 def test_schedule_model_detects_the_dropped_eager_claim():
