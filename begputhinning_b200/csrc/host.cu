@@ -573,7 +573,7 @@ static int enqueue_engine(bgt_batch *b, cudaStream_t st, bool capturing)
     if (e == cudaSuccess) e = launch_pack_all(b->d_insts, b->d_io, N, b->pack_words, b->bytes_only, st);
     if (e != cudaSuccess) return cuda_fail(e, "pack");
     sched_reset_kernel<<<std::min<unsigned>(1024, (b->cap + 255) / 256), 256, 0, st>>>(
-        b->d_sched, b->d_seq, b->d_item, b->cap, 20000000000LL, b->grid / 2);
+        b->d_sched, b->d_seq, b->d_item, b->cap, 20000000000LL, b->grid);
     stage_event(b->ev[1], st, capturing);
     e = launch_engine(b->grid, b->smem, b->d_insts, N, b->d_sched, st);
     if (e != cudaSuccess) return cuda_fail(e, "engine launch");

@@ -1125,9 +1125,10 @@ constexpr int kMaxClaim = 4;
 // instance's next wave.  The CTAs holding the tiles of a gang wave (a small
 // 3D wave whose tile list stays the same until the iteration ends) instead
 // meet at a per-instance barrier after each pass and go on with the same
-// tile; a budget of half the grid keeps enough CTAs outside gangs to claim
-// every gang's tiles, so no gang waits on a tile nobody can take.  Every
-// wait is bounded and reports a status bit.
+// tile.  A budget caps the tiles of all live gangs together at the number of
+// CTAs, so all gangs can be staffed at once; the CTAs outside gangs finish
+// their tiles and claim in ticket order, so no gang waits on a tile nobody
+// can take.  Every wait is bounded and reports a status bit.
 __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched *S, int box_words)
 {
     extern __shared__ __align__(128) uint32_t smem_raw[];

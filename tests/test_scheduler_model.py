@@ -44,7 +44,7 @@ class Model:
         self.items = [{}, {}]  # ticket -> (inst, tile, pass, n, gang)
         self.live = 0
         self.live_prio = [0, 0]
-        self.budget = grid // 2
+        self.budget = grid
         self.budget0 = self.budget
         self.producing = []  # pending item publications: (ring, ticket, item)
         self.eager_claim = False
@@ -264,11 +264,10 @@ def test_schedule_model_many_volumes_small_grid():
 
 
 @pytest.mark.parametrize("grid", [2, 4, 6])
-def test_schedule_model_any_budget_up_to_the_grid(grid):
-    # the engine reserves half the grid; the argument holds for any budget up
-    # to the grid (all live gangs together fit on the CTAs at once)
+def test_schedule_model_smaller_budgets(grid):
+    # the engine's budget is the whole grid; smaller ones only form fewer gangs
     for seed in range(15):
-        run_model(3000 + 7 * seed + grid, grid=grid, n2d=2, n3d=6, budget=grid)
+        run_model(3000 + 7 * seed + grid, grid=grid, n2d=2, n3d=6, budget=grid // 2)
 
 
 def test_schedule_model_detects_the_dropped_eager_claim():
