@@ -148,7 +148,7 @@ static int encode_map(CUtensorMap *m, const Inst &in, const int (&bx)[3], uint32
 }
 
 // ------------------------------------------------------------ autotune ----
-// Default tile configuration by shape; the autotuner (tune.cpp) may override
+// Default tile configuration by shape; the autotuner (begputhinning_b200/tune.py) may override
 // through bgt::tuned_cfg.
 int bgt::default_cfg(int dims, int W, int H, int D)
 {

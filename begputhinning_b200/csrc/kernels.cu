@@ -1175,16 +1175,15 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
                 for (int spin = 0;; spin++) {
                     unsigned t = 0;
                     int r = -1;
-                    const bool ring0_waiting =
-                        pend && (int)(ld_volatile_u(&S->ring[0].tail) - ld_volatile_u(&S->ring[0].head)) > 0;
-                    if (pend && !ring0_waiting) {  // next held ticket of the last multiple claim
+                    // held bulk tickets are consumed before anything else: a
+                    // CTA that took a ring-0 (gang) ticket while holding bulk
+                    // tickets could keep a 2D wave from finishing while its
+                    // gang waits for members the wave's waiters would supply
+                    if (pend) {  // next held ticket of the last multiple claim
                         r = 1;
                         t = pend_t;
                         pend -= 1;
                         pend_t = t + 1;
-                    } else if (ring0_waiting) {  // ring 0 first; the held ticket waits
-                        t = atomicAdd(&S->ring[0].head, 1u);
-                        r = 0;
                     } else {
                         // both rings' counters in one round trip; ring 0 first
                         const unsigned h0 = ld_volatile_u(&S->ring[0].head), t0 = ld_volatile_u(&S->ring[0].tail);
@@ -1241,8 +1240,7 @@ __global__ void __launch_bounds__(kThreads, 8) engine_kernel(Inst *insts, Sched 
         }
         parity ^= 1u;
         const uint32_t m = run_tile(in, q, tile, smem, &band);  // ends with a barrier: smem is free again
-        if (threadIdx.x == 32 && pend > 0 && !(gang_tile && q % 6 != 5) &&
-            (int)(ld_volatile_u(&S->ring[0].tail) - ld_volatile_u(&S->ring[0].head)) <= 0) {
+        if (threadIdx.x == 32 && pend > 0 && !(gang_tile && q % 6 != 5)) {
             // while thread 0 records this tile, stage the next held ticket's
             // tile if its item is already there (one look, no waiting)
             int4 it;

@@ -2,9 +2,9 @@
 //
 // Some callers of this library must not call cudaMalloc: plugins that run
 // inside a host application which owns all device memory through its own
-// pool, real-time loops where an allocation's implicit device
-// synchronisation would stall the frame, and code that records its work into
-// a CUDA graph, where cudaMalloc is not a capturable operation.  For them,
+// pool (an allocation behind the pool's back can fail or fragment it), and
+// real-time loops where an allocation's implicit device synchronisation
+// would stall the frame.  For them,
 // bgt_thin2d_device_noalloc thins one 2D image using only a fixed scratch
 // array compiled into the library: a file-scope __device__ array of
 // kNoAllocScratchBytes that every GPU which loads the library keeps until the
@@ -12,7 +12,8 @@
 // allocating library call); the caller passes the device input and output.
 //
 // The work is the plain path: pack, then one launch per pass with a readback
-// of the change flag after each pass, then unpack, all on the caller's stream.
+// of the change flag after each pass (the call synchronises the stream once
+// per pass), then unpack, all on the caller's stream.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -37,13 +38,25 @@ void *g_noalloc_ptr[kMaxDevices] = {};
 
 size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Keeps the calling thread's current device across the call: callers without
+// a context of their own rely on it staying where they put it.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() { cudaGetDevice(&prev); }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 using namespace bgt;
 
 // Thin a 2D image in device memory without allocating any device memory.
 // dtype, d_in and d_out as for bgt_thin2d_device; stream is a cudaStream_t
-// (NULL: the legacy default stream); device is made current for the call.
+// (NULL: the legacy default stream) of `device`, which is made current for
+// the call; the caller's current device is restored on return.
 //
 // Limits and sharing: the packed image (two copies, 2*ceil(width/32 rounded
 // up to 4)*height*4 bytes) plus small tables must fit in the 8 MiB array,
@@ -106,6 +119,7 @@ extern "C" int bgt_thin2d_device_noalloc(int device, int dtype, const void *d_in
                     width, height, need, kNoAllocScratchBytes);
 
     std::lock_guard<std::mutex> lock(g_noalloc_lock);
+    DeviceGuard keep_device;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     if (!g_noalloc_ptr[device]) {
@@ -150,7 +164,14 @@ extern "C" int bgt_thin2d_device_noalloc(int device, int dtype, const void *d_in
         e = launch_pack(dtype, 0, d_in, width, height, 1, width, height, 1, in.P, in.buf[0], in.buf[1], st);
     if (e == cudaSuccess) e = launch_tile_init(d_inst, in, nullptr, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_status, 0, sizeof(int), st);
-    if (e != cudaSuccess) return cuda_fail(e, "no-allocation set-up");
+    // Once work is queued, every return waits for it first (still holding
+    // the lock), so no kernel of this call can touch the shared array after
+    // the next caller has taken it.
+    auto fail_after_queue = [&](int rc) {
+        cudaStreamSynchronize(st);
+        return rc;
+    };
+    if (e != cudaSuccess) return fail_after_queue(cuda_fail(e, "no-allocation set-up"));
 
     int last_change = -1, converged = 0;
     for (int q = 0; q < in.pass_cap; q++) {
@@ -159,19 +180,19 @@ extern "C" int bgt_thin2d_device_noalloc(int device, int dtype, const void *d_in
         if (e == cudaSuccess) e = launch_plain_pass(cfg, d_inst, in.ntiles, q, d_flag, d_status, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&h_flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return cuda_fail(e, "no-allocation pass");
+        if (e != cudaSuccess) return fail_after_queue(cuda_fail(e, "no-allocation pass"));
         if (h_flag) last_change = q;
         if (q - last_change >= in.window) {
             converged = 1;
             break;
         }
     }
-    if (!converged) return fail(BGT_ERR_LIMIT, "hit the pass cap");
+    if (!converged) return fail_after_queue(fail(BGT_ERR_LIMIT, "hit the pass cap"));
     e = launch_unpack(dtype, in.buf[0], width, height, 1, in.P, d_out, st);
     int h_status = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_fail(e, "no-allocation unpack");
+    if (e != cudaSuccess) return fail_after_queue(cuda_fail(e, "no-allocation unpack"));
     if (h_status) return fail(BGT_ERR_TIMEOUT, "a device wait gave up (status bits 0x%x)", h_status);
     return BGT_OK;
 }

@@ -75,11 +75,13 @@ int bgt_thin3d_device(bgt_ctx *ctx, int dtype, const void *d_in, int width, int 
 
 /* ---- thinning without device allocation --------------------------------
  * No counterpart in the reference.  For callers that must not allocate
- * device memory (a host application that owns all device memory through its
- * own pool, a real-time loop that cannot afford an allocation's implicit
- * synchronisation, work being recorded into a CUDA graph): thins one 2D
- * image of `dtype` from d_in to d_out (device buffers, width*height pixels)
- * on `stream` (a cudaStream_t, NULL = legacy default stream) of `device`,
+ * device memory (a plugin inside a host application that owns all device
+ * memory through its own pool, a real-time loop that cannot afford an
+ * allocation's implicit synchronisation): thins one 2D image of `dtype`
+ * from d_in to d_out (device buffers, width*height pixels) on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) of `device` (the caller's
+ * current device is restored on return), synchronising the stream once
+ * per pass,
  * using only an 8 MiB scratch array compiled into the library (kept by
  * every GPU that loads it until the process exits).  Images whose packed
  * form does not fit (beyond about 4096 x 4096) are rejected with

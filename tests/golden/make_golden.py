@@ -1,7 +1,7 @@
 """Generate the golden vectors in tests/golden/ from the reference's own code.
 
 Runs only where the reference tree is present (it loads oracle/_ref, built by
-``make -C oracle ref`` from the reference sources: the reference's rule
+``make -C oracle ref REF=<reference tree>`` from the reference sources: the reference's rule
 functions run by a global synchronous host driver, its ExtractSegmentsV and
 its CenterlineExtraction).  Inputs are seeded and stored with the outputs, so
 the tests need neither the generator nor the reference.

@@ -48,6 +48,7 @@ class Model:
         self.budget0 = self.budget
         self.producing = []  # pending item publications: (ring, ticket, item)
         self.eager_claim = False
+        self.held_first = True
 
     def next_wave(self, ii, q1):
         """The wave of pass q1 of instance ii: reserve its tickets at once
@@ -94,6 +95,7 @@ class CTA:
         self.take = None
         self.eager = None
         self.finished = False
+        self.held_first = m.held_first
 
     def depth(self, r):
         return self.m.tail[r] - self.m.head[r]
@@ -114,7 +116,11 @@ class CTA:
             # a later one, so other CTAs may take tickets in between (a ticket
             # can then lie past the tail and wait for a later wave)
             d0, d1 = self.depth(0), self.depth(1)
-            ring0_waiting = self.pend > 0 and d0 > 0
+            # the engine consumes its held bulk tickets before taking a ring-0
+            # ticket, so a CTA never joins a gang while it holds tickets that
+            # other instances' waves wait for (held_first = False models the
+            # earlier rule, which let ring 0 jump ahead of held tickets)
+            ring0_waiting = self.pend > 0 and d0 > 0 and not self.held_first
             if self.pend > 0 and not ring0_waiting:
                 self.ticket = (1, self.pend_t)
                 self.pend -= 1
@@ -163,7 +169,7 @@ class CTA:
             inst.seen.setdefault(q, []).append(tile)
             assert inst.seen[q].count(tile) == 1, "tile processed twice in one pass"
             # thread 32: one look at the next held ticket
-            if self.pend > 0 and not (gang and q % 6 != 5) and self.depth(0) <= 0:
+            if self.pend > 0 and not (gang and q % 6 != 5) and (self.held_first or self.depth(0) <= 0):
                 if self.pend_t in m.items[1]:
                     self.ngot = m.items[1].pop(self.pend_t)
                     self.pend -= 1
@@ -282,3 +288,58 @@ def test_schedule_model_detects_the_dropped_eager_claim():
             assert "stuck" in str(e) or "did not finish" in str(e)
             stuck += 1
     assert stuck > 0
+
+
+def run_gang_vs_held_tickets(seed, held_first, grid=4):
+    """A 2D instance whose waves (8 tiles on 4 CTAs) are deep enough for
+    multiple claims, and a volume whose waves of 4 tiles form gangs as large
+    as the whole grid, published at a random early step.  Returns False when
+    the schedule gets stuck."""
+    rng = random.Random(seed)
+    a = Inst(rng, 2)
+    a.waves = [8, 8, 8, 0]
+    v = Inst(rng, 3)
+    v.waves = [4] * 12 + [0]
+    m = Model(rng, [a, v], grid)
+    m.held_first = held_first
+    for inst in m.insts:
+        m.live += 1
+        m.live_prio[inst.prio] += 1
+    m.next_wave(0, 0)
+    ctas = [CTA(m) for _ in range(grid)]
+    publish_at = rng.randint(0, 30)
+    published = False
+    idle = 0
+    for step in range(20000):
+        if not published and step == publish_at:
+            m.next_wave(1, 0)
+            published = True
+        progress = m.publish_one() if rng.random() < 0.5 else False
+        order = list(range(grid))
+        rng.shuffle(order)
+        for c in order[: rng.randint(1, grid)]:
+            progress |= ctas[c].step()
+        if all(c.finished for c in ctas):
+            return True
+        if progress:
+            idle = 0
+            continue
+        if not published:
+            m.next_wave(1, 0)
+            published = True
+            continue
+        progress = m.publish_one() or any(c.step() for c in ctas)
+        idle = 0 if progress else idle + 1
+        if idle >= 3:
+            return False
+    raise AssertionError("model did not finish within its step limit")
+
+
+def test_gang_never_waits_on_a_ticket_holder():
+    """A CTA holding bulk tickets used to be able to take a gang ticket first
+    (ring 0 had priority over its held tickets); the 2D wave behind a held
+    ticket then never finished while the gang waited for members.  The
+    engine now consumes held tickets first: no interleaving gets stuck, and
+    the model still finds the stall under the earlier rule."""
+    assert all(run_gang_vs_held_tickets(s, held_first=True) for s in range(1500))
+    assert not all(run_gang_vs_held_tickets(s, held_first=False) for s in range(1500))

@@ -1,17 +1,19 @@
 """The no-allocation thinning entry point (bgt_thin2d_device_noalloc).
 
-It serves callers that cannot allocate device memory (an application that
-owns all device memory through its own pool, a real-time loop, work being
-captured into a CUDA graph), so it runs on a scratch array compiled into the
-library.  This test calls it through the C ABI twice in a row, on different
-images, and checks each output bit for bit (thinning is integer work, the
-tolerance is zero) against the allocating entry point bgt_thin2d_device.
-The file is named to be collected last."""
+It serves callers that cannot allocate device memory (a plugin inside an
+application that owns all device memory through its own pool, a real-time
+loop that cannot afford an allocation's implicit synchronisation), so it
+runs on a scratch array compiled into the library.  This test calls it
+through the C ABI twice in a row, on different images, and checks each
+output bit for bit (thinning is integer work, the tolerance is zero)
+against the allocating entry point bgt_thin2d_device and against the
+oracle.  The file is named to be collected last."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
+from oracle import pyoracle as po
 from tests.helpers import blobs2d
 
 pytestmark = pytest.mark.gpu
@@ -44,6 +46,7 @@ def test_noalloc_matches_allocating_path():
         assert rc == 0, lib().bgt_last_error()
         want = _reference_thin(ctx, t)
         assert torch.equal(out, want), f"shape {img.shape}: {(out != want).sum().item()} pixels differ"
+        assert np.array_equal(out.cpu().numpy(), po.thin2d(img)[0]), f"shape {img.shape}: differs from the oracle"
     ctx.close()
 
 
