@@ -19,6 +19,7 @@ EXPORTS = [
     "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
     "bgt_batch_reserve", "bgt_batch_reset", "bgt_batch_set_grid",
     "bgt_batch_set_io", "bgt_batch_run", "bgt_batch_instance_stats", "bgt_batch_device_bytes", "bgt_batch_work", "bgt_batch_stage_ms",
+    "bgt_batch_engine_ms", "bgt_batch_set_engine", "bgt_batch_plan",
     "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe", "bgt_rule_table",
     "bgt_server_create", "bgt_server_submit", "bgt_server_poll", "bgt_server_drain", "bgt_server_stats",
     "bgt_server_reset_stats", "bgt_server_destroy",
@@ -77,6 +78,9 @@ def _declare(L):
         "bgt_batch_device_bytes": [vp, C.POINTER(C.c_size_t)],
         "bgt_batch_work": [vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)],
         "bgt_batch_stage_ms": [vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)],
+        "bgt_batch_engine_ms": [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)],
+        "bgt_batch_set_engine": [vp, I],
+        "bgt_batch_plan": [vp, I, ip, ip],
         "bgt_tune_class": [I, I, I, I],
         "bgt_tune_set": [I, I, I],
         "bgt_tune_get": [I, I, ip],

@@ -275,6 +275,19 @@ class Batch:
         call before finalize()."""
         check(lib().bgt_batch_set_grid(self.h, ctas))
 
+    def set_engine(self, rings_only: bool) -> None:
+        """Thin every instance with the tile rings (True) or let the
+        resident kernel take every instance that fits (False, the default);
+        call before finalize()."""
+        check(lib().bgt_batch_set_engine(self.h, 1 if rings_only else 0))
+
+    def plan(self, i: int):
+        """(resident, bands): whether the resident kernel takes instance i
+        and how many CTAs a 2D image is cut into."""
+        r, n = C.c_int(), C.c_int()
+        check(lib().bgt_batch_plan(self.h, i, C.byref(r), C.byref(n)))
+        return bool(r.value), n.value
+
     def finalize(self) -> None:
         check(lib().bgt_batch_finalize(self.h))
 
@@ -312,6 +325,12 @@ class Batch:
         a, b, c = C.c_float(), C.c_float(), C.c_float()
         check(lib().bgt_batch_stage_ms(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
+
+    def engine_ms(self):
+        """(resident kernel, tile rings) device milliseconds of the last engine run."""
+        a, b = C.c_float(), C.c_float()
+        check(lib().bgt_batch_engine_ms(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def device_bytes(self) -> int:
         n = C.c_size_t()

@@ -22,7 +22,7 @@ BUILD = os.path.join(ROOT, "_build")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["kernels.cu", "host.cu", "segments.cu", "centerline.cu", "noalloc.cu", "serve.cu"]
+CU_SOURCES = ["kernels.cu", "resident.cu", "host.cu", "segments.cu", "centerline.cu", "noalloc.cu", "serve.cu"]
 CXX_SOURCES = ["dropin.cpp"]
 HEADERS = ["common.cuh", "rules.cuh", "tiles.cuh", "kernels.cuh", "host.h"]
 

@@ -64,6 +64,11 @@ struct alignas(16) Inst {
     int gang;                 // 3D: gang arrivals so far (barrier between the gang's passes)
     unsigned long long tiles_run;   // tiles processed (skipped tiles excluded)
     unsigned long long work_words;  // packed core words processed (sum over passes and tiles)
+    // resident engine (resident.cu)
+    int res;                  // 1: thinned by the resident engine, 0: by the tile rings
+    int spill;                // set by the resident engine when a volume's bricks do not fit: the rings take it
+    int res_arrive;           // arrivals at the band barrier of a multi-CTA image (all bands, all passes)
+    int res_last;             // last pass in which some band's core changed (-1: none yet)
 };
 
 // Core words of a tile (clamped to the image): the algorithmic unit of a pass.

@@ -2,6 +2,8 @@
 // TMA tensor maps, the persistent engine and the plain per-pass path, CUDA
 // graph replay) and the drop-in thinning entry points.
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -212,6 +214,7 @@ static int batch_add(bgt_batch *b, int dims, int W, int H, int D, int cfg, int *
     it.H = H;
     it.D = D;
     it.cfg = cfg;
+    it.auto_cfg = cfg < 0;
     b->items.push_back(it);
     if (id) *id = (int)b->items.size() - 1;
     return BGT_OK;
@@ -224,6 +227,72 @@ extern "C" int bgt_batch_add3d(bgt_batch *b, int w, int h, int d, int cfg, int *
 }
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Which instances the resident engine takes and how large 2D images are cut
+// into bands: a band holds at most what one CTA's shared memory does, and an
+// image is cut further while it is a large share of the batch's work (so a
+// batch of few large images still spreads over the SMs), keeping at least 32
+// core rows per band.  Items are ordered volumes first (largest first: their
+// chains of iterations are the longest), then images largest first, the bands
+// of one image consecutive.
+static void plan_resident(bgt_batch *b)
+{
+    constexpr int kHalo = 4, kMinCore = 32;
+    b->res_items.clear();
+    b->any_ring = false;
+    b->any_res3d = false;
+    const int N = (int)b->items.size();
+    const bool rings_only = b->engine_mode == 1 || (getenv("BGT_ENGINE") && !strcmp(getenv("BGT_ENGINE"), "rings"));
+    double total = 0;
+    for (const BatchItem &it : b->items) total += (double)((it.W + 31) / 32) * it.H * it.D;
+    const double target = std::max(total / std::max(1, b->res_grid), 4096.0);
+    std::vector<std::pair<double, int>> vols, imgs;
+    for (int i = 0; i < N; i++) {
+        const BatchItem &it = b->items[i];
+        Inst &in = b->h[i];
+        in.res = 0;
+        if (rings_only || !it.auto_cfg || b->res_grid < 1) continue;
+        if (it.dims == 3) {
+            if (!res_fits3d(it.W, it.H, it.D)) continue;
+            in.res = 1;
+            vols.push_back({(double)it.W * it.H * it.D, i});
+        } else {
+            in.res = 1;
+            imgs.push_back({(double)((it.W + 31) / 32) * it.H, i});
+        }
+    }
+    std::stable_sort(vols.begin(), vols.end(), [](auto &x, auto &y) { return x.first > y.first; });
+    std::stable_sort(imgs.begin(), imgs.end(), [](auto &x, auto &y) { return x.first > y.first; });
+    for (auto &v : vols) {
+        b->res_items.push_back(ResItem{v.second, 0, 1, 0, 0, 0});
+        b->any_res3d = true;
+    }
+    for (auto &m : imgs) {
+        const int i = m.second;
+        const BatchItem &it = b->items[i];
+        const int fit = res_rows_fit2d(it.W);
+        int G = 1;
+        if (it.H > fit) {
+            G = (it.H + (fit - 2 * kHalo) - 1) / std::max(1, fit - 2 * kHalo);
+            while ((it.H + G - 1) / G + 2 * kHalo > fit) G++;
+        }
+        const int G_work = (int)std::ceil(m.first / target);
+        const int G_rows = std::max(1, it.H / kMinCore);
+        G = std::max(G, std::min(G_work, G_rows));
+        G = std::min(G, b->res_grid);
+        const bool fits = G == 1 ? it.H <= fit : (it.H + G - 1) / G + 2 * kHalo <= fit && it.H / G >= kHalo;
+        if (!fits) {
+            b->h[i].res = 0;  // cannot be cut into bands that fit: the rings take it
+            continue;
+        }
+        for (int k = 0; k < G; k++) {
+            const int r0 = (int)((long long)k * it.H / G), r1 = (int)((long long)(k + 1) * it.H / G);
+            b->res_items.push_back(ResItem{i, k, G, r0, r1, G > 1 ? kHalo : 0});
+        }
+    }
+    for (int i = 0; i < N; i++)
+        if (!b->h[i].res) b->any_ring = true;
+}
 
 extern "C" int bgt_batch_finalize(bgt_batch *b)
 {
@@ -293,6 +362,16 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     const size_t off_inst = off; off = align_up(off + (size_t)N * sizeof(Inst), 256);
     const size_t off_tmap = off; off = align_up(off + (size_t)N * kMapsPerInst * sizeof(CUtensorMap), 256);
     const size_t off_flag = off; off = align_up(off + 64, 256);
+    // resident engine: item list (at most one band per row of every image) + its scheduler
+    {
+        int per_sm = 0;
+        if (res_occupancy(&per_sm) == cudaSuccess && per_sm > 0) b->res_grid = b->ctx->sms * per_sm;
+        else b->res_grid = 0;
+        if (b->grid_cap > 0) b->res_grid = std::min(b->res_grid, b->grid_cap);
+    }
+    plan_resident(b);
+    const size_t off_res = off; off = align_up(off + std::max<size_t>(1, b->res_items.size()) * sizeof(ResItem), 256);
+    const size_t off_rs = off; off = align_up(off + sizeof(ResSched), 256);
     cudaError_t e;
     if (b->reserved) {
         // a reserved pool is re-laid-out for every set of instances, never reallocated
@@ -313,6 +392,8 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     b->d_flag = (int *)(P + off_flag);
     b->d_lc = P + off_lc;
     b->d_io = (IODesc *)(P + off_io);
+    b->d_res_items = (ResItem *)(P + off_res);
+    b->d_rs = (ResSched *)(P + off_rs);
     b->cap = cap;
     std::vector<CUtensorMap> &maps = b->maps;
     maps.assign((size_t)N * kMapsPerInst, CUtensorMap());
@@ -341,6 +422,9 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     e = cudaMemcpyAsync(b->d_tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_insts, b->h.data(), (size_t)N * sizeof(Inst), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !b->res_items.empty())
+        e = cudaMemcpyAsync(b->d_res_items, b->res_items.data(), b->res_items.size() * sizeof(ResItem),
+                            cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
         if (!b->reserved) batch_free_device(b);
         return cuda_fail(e, "batch table upload");
@@ -424,16 +508,57 @@ extern "C" int bgt_batch_stage_ms(bgt_batch *b, float *pack_ms, float *engine_ms
 {
     if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
     if (b->last_mode != 0) return fail(BGT_ERR_STATE, "stage times exist only for engine runs");
-    cudaError_t e = cudaEventSynchronize(b->ev[3]);
+    cudaError_t e = cudaEventSynchronize(b->ev[4]);
     if (e != cudaSuccess) return cuda_fail(e, "event sync");
-    float t[3] = {0, 0, 0};
-    for (int k = 0; k < 3; k++) {
+    float t[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; k++) {
         e = cudaEventElapsedTime(&t[k], b->ev[k], b->ev[k + 1]);
         if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
     }
     if (pack_ms) *pack_ms = t[0];
-    if (engine_ms) *engine_ms = t[1];
-    if (unpack_ms) *unpack_ms = t[2];
+    if (engine_ms) *engine_ms = t[1] + t[2];
+    if (unpack_ms) *unpack_ms = t[3];
+    return BGT_OK;
+}
+
+// The engine stage of the last run split into the resident kernel and the
+// tile-ring engine that follows it (volumes that spilled, instances the
+// resident engine does not take).
+extern "C" int bgt_batch_engine_ms(bgt_batch *b, float *resident_ms, float *rings_ms)
+{
+    if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    if (b->last_mode != 0) return fail(BGT_ERR_STATE, "stage times exist only for engine runs");
+    cudaError_t e = cudaEventSynchronize(b->ev[4]);
+    if (e != cudaSuccess) return cuda_fail(e, "event sync");
+    float r = 0, g = 0;
+    e = cudaEventElapsedTime(&r, b->ev[1], b->ev[2]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&g, b->ev[2], b->ev[3]);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
+    if (resident_ms) *resident_ms = r;
+    if (rings_ms) *rings_ms = g;
+    return BGT_OK;
+}
+
+// Engine choice for the next finalize: 0 = resident engine where an instance
+// fits (the default), 1 = tile rings only.
+extern "C" int bgt_batch_set_engine(bgt_batch *b, int mode)
+{
+    if (!b || mode < 0 || mode > 1) return fail(BGT_ERR_ARG, "bad argument");
+    b->engine_mode = mode;
+    return BGT_OK;
+}
+
+// How the last finalize planned instance `id`: *resident = 1 when the
+// resident engine takes it, *bands = the number of bands of a 2D image.
+extern "C" int bgt_batch_plan(bgt_batch *b, int id, int *resident, int *bands)
+{
+    if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    if (id < 0 || id >= (int)b->items.size()) return fail(BGT_ERR_ARG, "bad instance id");
+    int n = 0;
+    for (const ResItem &r : b->res_items)
+        if (r.inst == id) n++;
+    if (resident) *resident = b->h[id].res;
+    if (bands) *bands = n;
     return BGT_OK;
 }
 
@@ -575,14 +700,22 @@ static int enqueue_engine(bgt_batch *b, cudaStream_t st, bool capturing)
     sched_reset_kernel<<<std::min<unsigned>(1024, (b->cap + 255) / 256), 256, 0, st>>>(
         b->d_sched, b->d_seq, b->d_item, b->cap, 20000000000LL, b->grid);
     stage_event(b->ev[1], st, capturing);
-    e = launch_engine(b->grid, b->smem, b->d_insts, N, b->d_sched, st);
-    if (e != cudaSuccess) return cuda_fail(e, "engine launch");
+    // bands of an image wait for one another only for the length of one
+    // iteration of the slowest band: 4 s is far beyond any legitimate wait
+    e = launch_resident(b->res_grid, b->d_insts, N, b->d_res_items, (int)b->res_items.size(), b->d_rs,
+                        4000000000LL, st);
+    if (e != cudaSuccess) return cuda_fail(e, "resident engine launch");
     stage_event(b->ev[2], st, capturing);
+    if (b->any_ring || b->any_res3d) {
+        e = launch_engine(b->grid, b->smem, b->d_insts, N, b->d_sched, st);
+        if (e != cudaSuccess) return cuda_fail(e, "engine launch");
+    }
+    stage_event(b->ev[3], st, capturing);
     if (b->any_out) {
         e = launch_unpack_all(b->d_insts, b->d_io, N, b->unpack_words, st);
         if (e != cudaSuccess) return cuda_fail(e, "unpack");
     }
-    stage_event(b->ev[3], st, capturing);
+    stage_event(b->ev[4], st, capturing);
     return BGT_OK;
 }
 
@@ -689,9 +822,12 @@ int bgt::batch_check(bgt_batch *b)
 {
     cudaError_t e = cudaStreamSynchronize(b->ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "batch run");
-    int status = 0;
+    int status = 0, rstatus = 0;
     e = cudaMemcpy(&status, &b->d_sched->status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && b->last_mode == 0 && !b->res_items.empty())
+        e = cudaMemcpy(&rstatus, &b->d_rs->status, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "status readback");
+    status |= rstatus;
     if (status & (kErrTmaTimeout | kErrQueueTimeout | kErrQueueFull))
         return fail(BGT_ERR_TIMEOUT, "device wait gave up (status bits 0x%x)", status);
     if (status & kErrPassLimit) return fail(BGT_ERR_LIMIT, "an instance hit the pass cap");

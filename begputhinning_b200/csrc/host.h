@@ -25,6 +25,7 @@ struct Scratch {
 
 struct BatchItem {
     int dims = 2, W = 0, H = 0, D = 1, cfg = -1;
+    bool auto_cfg = true;  // added with cfg < 0 (the resident engine may take it)
 };
 
 struct IO {
@@ -113,7 +114,16 @@ struct bgt_batch {
     unsigned cap = 0;
     int smem = 0;
     int grid = 0;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // stage boundaries of an engine run
+    // stage boundaries of an engine run: pack, resident engine, tile engine, unpack
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // resident engine plan (resident.cu): items in the order they are taken
+    int engine_mode = 0;              // 0: resident engine where it fits, tile rings for the rest; 1: rings only
+    std::vector<bgt::ResItem> res_items;
+    bgt::ResItem *d_res_items = nullptr;
+    bgt::ResSched *d_rs = nullptr;
+    int res_grid = 0;
+    bool any_ring = false;            // some instance is planned for the tile rings
+    bool any_res3d = false;           // some volume may spill from the resident engine to the rings
     cudaGraphExec_t gexec = nullptr;
     bool graph_valid = false;
 };

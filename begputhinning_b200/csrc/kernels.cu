@@ -1046,6 +1046,8 @@ __global__ void __launch_bounds__(kThreads) engine_seed_kernel(Inst *insts, int 
 {
     __shared__ uint32_t scratch[2048];
     for (int ii = blockIdx.x; ii < ninst; ii += gridDim.x) {
+        // instances of the resident engine are done unless they spilled
+        if (insts[ii].res && !insts[ii].spill) continue;
         if (threadIdx.x == 0) {
             insts[ii].converged = 0;
             insts[ii].passes_run = 0;

@@ -46,6 +46,34 @@ struct Sched {
     long long timeout_ns;
 };
 
+// Resident engine (resident.cu).  A work item is one instance, or one band
+// of rows of a 2D image too large for one CTA (the bands of an image run
+// together and trade `halo` boundary rows through global memory after every
+// iteration).  Items are taken in order by one fetch-and-add.
+struct ResItem {
+    int inst;        // instance index
+    int band, bands; // band index and number of bands (1: the whole instance)
+    int r0, r1;      // 2D: core rows [r0, r1) of the band
+    int halo;        // 2D: halo rows kept on each side of the core (0 for a single band)
+};
+struct ResSched {
+    int head;        // next item
+    int nitems;
+    int status;      // error bits
+    int pad;
+    long long timeout_ns;
+};
+constexpr int kResThreads = 512;
+// Dynamic shared memory of the resident kernel (one CTA per SM).
+int res_smem_bytes();
+// Rows of a W-wide 2D band (core plus halo) that one CTA holds.
+int res_rows_fit2d(int W);
+// Whether a D x H x W volume's brick table fits (its bricks are counted on the device).
+bool res_fits3d(int W, int H, int D);
+cudaError_t res_occupancy(int *per_sm);  // resident CTAs per SM
+cudaError_t launch_resident(int grid, Inst *d_insts, int ninst, const ResItem *d_items, int nitems,
+                            ResSched *d_rs, long long timeout_ns, cudaStream_t st);
+
 // Per-instance input/output of a batch-wide pack/unpack launch.
 // Unsigned 32-bit division by a divisor fixed per instance, as a multiply
 // and shifts (Granlund and Montgomery, "Division by invariant integers using

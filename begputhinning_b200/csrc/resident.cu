@@ -1,0 +1,789 @@
+// resident.cu -- the resident engine: every work item (an instance, or one
+// band of rows of a 2D image too large for one CTA) is loaded once into one
+// CTA's shared memory and thinned there from its first subiteration to its
+// fixed point; only the bands of a large image meet, once per iteration, to
+// trade boundary rows through global memory.  One CTA of 512 threads per SM
+// holds up to 225 KB.
+//
+// 2D band (dense).  Rows of the band (core plus `halo` rows on each side,
+// clamped to the image) lie in shared memory with an odd pitch of
+// 2*ceil(wl/2)+3 words (wl = ceil(W/32); a zero word left of every row and
+// zero words right of it).  A subiteration processes strips of 32 rows, one
+// warp per strip, lane = row, walking the row in pairs of words: each lane
+// loads its own row and the rows above and below straight from shared
+// memory and forms the x-neighbours by funnel shifts.  Rows are updated in
+// place: within a warp the loads of a step precede its stores (__syncwarp),
+// and the rows just outside a strip (read by its lanes 0 and 31) come from a
+// copy of every strip's first and last rows taken at the end of the previous
+// subiteration (double-buffered by parity), so no warp reads a row another
+// warp is rewriting.  A strip whose neighbourhood (itself and the strips above
+// and below) did not change during the last four subiterations -- one of
+// each direction -- is a fixed point for the next one and is skipped.  A
+// single band stops after four consecutive subiterations without a deletion
+// (a fixed point of N, S, E and W: the reference's result, whatever the
+// alignment).  Bands of one image run their iterations (N, S, E, W) in
+// lockstep: after each iteration a band writes its first and last `halo`
+// core rows to global memory, meets the other bands at a per-image counter,
+// stops if no band's core changed in that iteration, and otherwise reads its
+// halo rows from its neighbours.  With halo = 4 rows, wrong values entering
+// at a band's outer edge during an iteration reach at most its halo rows.
+//
+// 3D volume (sparse bricks, one CTA).  Deletion never adds foreground, so
+// bricks of 32 voxels (one word) x 32 rows x 4 planes that are empty at the
+// start stay empty.  Only the non-empty ones are stored: a brick table maps
+// each brick to a slot (0: the all-zero brick), and three slot buffers hold
+// the state (ping-pong) and the iteration's pre-test union.  A warp
+// processes a brick, lane = row, marching through its four planes with a
+// three-plane window of 3x3 (row, word) neighbourhoods loaded from the
+// neighbouring bricks' slots.  Brick activity follows the iteration: a brick
+// whose 3x3x3 brick neighbourhood did not change during the previous
+// iteration has an empty union and cannot change (the argument of the tile
+// engine), so only active bricks are processed.  A volume whose non-empty
+// bricks do not fit is flagged `spill` and left to the tile engine.
+//
+// Rules, order of directions and termination are those of the tile engine
+// (2D/CUDA_ThinningKernelMultiBlock2D.cuh:104-135,
+// 3D/CUDA_ThinningKernel3D_Linear.cuh:746-782); every wait is bounded.
+#include <algorithm>
+
+#include "kernels.cuh"
+#include "rules.cuh"
+
+namespace bgt {
+
+namespace {
+constexpr int kWarps = kResThreads / 32;
+constexpr int kSmemBytes = 230400;   // dynamic shared memory per CTA
+constexpr int kLongAgo = -(1 << 29); // "last change" of a strip that never changed
+constexpr int kSlotWords = 129;      // 4 planes x 32 rows, plus one word so slots fall on different banks
+constexpr int kMaxBricks = 16384;    // brick table entries of a resident volume
+constexpr int kBZ = 4;               // planes per brick
+
+__host__ __device__ inline size_t up16(size_t v) { return (v + 15) & ~size_t(15); }
+}  // namespace
+
+// ------------------------------------------------------------ geometry ----
+__host__ __device__ inline int res_pitch2d(int W)
+{
+    const int wl = (W + 31) >> 5;
+    return 2 * ((wl + 1) >> 1) + 3;
+}
+
+// words of shared memory a band of nrows rows needs: zero row, rows, edge
+// copies (2 parities x 2 rows per strip) and the per-strip change record
+__host__ __device__ inline size_t res_words2d(int W, int nrows)
+{
+    const int pp = res_pitch2d(W);
+    const int ns = (nrows + 31) >> 5;
+    return (size_t)pp * (1 + (size_t)nrows + 4 * (size_t)ns) + (size_t)ns;
+}
+
+// bytes of shared memory a volume with nb bricks of which ns are non-empty needs
+__host__ __device__ inline size_t res_bytes3d(int nb, int ns)
+{
+    return up16((size_t)nb * 2) + up16((size_t)(ns + 1) * 4) + up16((size_t)(ns + 1) * 3) +
+           up16((size_t)(ns + 1) * 2) + (size_t)3 * (ns + 1) * kSlotWords * 4;
+}
+
+int res_smem_bytes() { return kSmemBytes; }
+
+int res_rows_fit2d(int W)
+{
+    int lo = 0, hi = 32767;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (res_words2d(W, mid) * 4 <= (size_t)kSmemBytes) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+bool res_fits3d(int W, int H, int D)
+{
+    const long long nb = (long long)((W + 31) / 32) * ((H + 31) / 32) * ((D + kBZ - 1) / kBZ);
+    return nb <= kMaxBricks && res_bytes3d((int)nb, 1) <= (size_t)kSmemBytes;
+}
+
+// ------------------------------------------------------------ helpers -----
+__device__ __forceinline__ bool res_wait_at_least(const int *p, int target, long long timeout_ns)
+{
+    const unsigned long long t_end = globaltimer() + (unsigned long long)timeout_ns;
+    for (int spin = 0;; spin++) {
+        if (ld_acquire(p) >= target) return true;
+        if ((spin & 63) == 63 && globaltimer() > t_end) return false;
+        __nanosleep(spin < 16 ? 32 : 128);
+    }
+}
+
+// Next work unit of a subiteration for this warp (dynamic distribution over
+// the CTA's warps): lane 0 takes a ticket of counter `c`.
+__device__ __forceinline__ int res_take(int *c)
+{
+    int k = 0;
+    if ((threadIdx.x & 31) == 0) k = atomicAdd(c, 1);
+    return __shfl_sync(kFull, k, 0);
+}
+
+// Exclusive prefix sum over the CTA of one int per thread; *total gets the sum.
+__device__ int res_block_exscan(int v, int *total)
+{
+    __shared__ int warp_sum[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();
+    int before = 0, all = 0;
+    for (int w = 0; w < kWarps; w++) {
+        const int s = warp_sum[w];
+        if (w < warp) before += s;
+        all += s;
+    }
+    __syncthreads();
+    *total = all;
+    return before + x - v;
+}
+
+// ------------------------------------------------------------ 2D ----------
+struct Band2D {
+    uint32_t *zero;     // pp zero words
+    uint32_t *rows;     // nrows x pp
+    uint32_t *E;        // [2 parities][nstrips][first, last row][pp]
+    int *lastchg;       // per strip: last subiteration with a deletion
+    int pp, npairs, wl, nrows, nstrips;
+    int a;              // image row of the band's first row in shared memory
+    int r0, r1;         // core rows (image coordinates)
+};
+
+// One subiteration of direction DIR on one strip's row (this lane's), in
+// place.  own/up/dn: this row and the rows above and below (pass-start
+// values; the row pointers of lanes 0 and 31 point at edge copies).  Words
+// 0 and 2*npairs+1.. are zero pads.  Returns the deleted bits.
+template <int DIR>
+__device__ __forceinline__ uint32_t res_row2d(uint32_t *own, const uint32_t *up, const uint32_t *dn, bool store,
+                                              int npairs)
+{
+    uint32_t ao = own[0], bo = own[1], au = up[0], bu = up[1], ad = dn[0], bd = dn[1];
+    uint32_t chg = 0;
+    for (int k = 0; k < npairs; k++) {
+        const int j = 2 * k + 1;
+        const uint32_t co = own[j + 1], eo = own[j + 2];
+        const uint32_t cu = up[j + 1], eu = up[j + 2];
+        const uint32_t cd = dn[j + 1], ed = dn[j + 2];
+        if (__any_sync(kFull, (bo | co) != 0u)) {
+            uint32_t X[8];
+            X[0] = bu;
+            X[1] = at_xp1(bu, cu);
+            X[2] = at_xp1(bo, co);
+            X[3] = at_xp1(bd, cd);
+            X[4] = bd;
+            X[5] = at_xm1(bd, ad);
+            X[6] = at_xm1(bo, ao);
+            X[7] = at_xm1(bu, au);
+            const uint32_t n0 = bo & ~rule2d<DIR>(X);
+            uint32_t Y[8];
+            Y[0] = cu;
+            Y[1] = at_xp1(cu, eu);
+            Y[2] = at_xp1(co, eo);
+            Y[3] = at_xp1(cd, ed);
+            Y[4] = cd;
+            Y[5] = at_xm1(cd, bd);
+            Y[6] = at_xm1(co, bo);
+            Y[7] = at_xm1(cu, bu);
+            const uint32_t n1 = co & ~rule2d<DIR>(Y);
+            __syncwarp();  // every lane has read words j .. j+2 of its neighbours' rows
+            if (store) {
+                own[j] = n0;
+                own[j + 1] = n1;
+            }
+            chg |= (n0 ^ bo) | (n1 ^ co);
+        }
+        ao = co;
+        bo = eo;
+        au = cu;
+        bu = eu;
+        ad = cd;
+        bd = ed;
+    }
+    return chg;
+}
+
+__device__ __forceinline__ void res_copy_edges2d(const Band2D &b, uint32_t *En, int s)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t *top = b.rows + (size_t)(32 * s) * b.pp;
+    const uint32_t *bot = b.rows + (size_t)min(32 * s + 31, b.nrows - 1) * b.pp;
+    uint32_t *et = En + (size_t)(2 * s) * b.pp, *eb = et + b.pp;
+    for (int w = lane; w < b.pp; w += 32) {
+        et[w] = top[w];
+        eb[w] = bot[w];
+    }
+}
+
+// One subiteration t (direction DIR = t % 4) over the band's strips.
+// Returns this thread's deleted core bits; adds processed words to *words.
+template <int DIR>
+__device__ uint32_t res_subit2d(const Band2D &b, int t, int *take, unsigned long long *words)
+{
+    const int lane = threadIdx.x & 31;
+    const size_t par = (size_t)2 * b.nstrips * b.pp;
+    const uint32_t *Ec = b.E + (t & 1) * par;
+    uint32_t *En = b.E + ((t + 1) & 1) * par;
+    uint32_t core = 0;
+    for (;;) {
+        const int s = res_take(take);
+        if (s >= b.nstrips) break;
+        const int lc = max(b.lastchg[s], max(s > 0 ? b.lastchg[s - 1] : kLongAgo,
+                                             s + 1 < b.nstrips ? b.lastchg[s + 1] : kLongAgo));
+        if (lc >= t - 4) {
+            const int r = 32 * s + lane;
+            const bool valid = r < b.nrows;
+            uint32_t *own = valid ? b.rows + (size_t)r * b.pp : b.zero;
+            const uint32_t *up = lane == 0 ? (s > 0 ? Ec + (size_t)(2 * s - 1) * b.pp : b.zero)
+                                           : (r - 1 < b.nrows ? b.rows + (size_t)(r - 1) * b.pp : b.zero);
+            const uint32_t *dn = lane == 31 ? (s + 1 < b.nstrips ? Ec + (size_t)(2 * s + 2) * b.pp : b.zero)
+                                            : (r + 1 < b.nrows ? b.rows + (size_t)(r + 1) * b.pp : b.zero);
+            const uint32_t chg = res_row2d<DIR>(own, up, dn, valid, b.npairs);
+            if (__any_sync(kFull, chg != 0u) && lane == 0) b.lastchg[s] = t;
+            const int gy = b.a + r;
+            if (valid && gy >= b.r0 && gy < b.r1) core |= chg;
+            if (lane == 0) *words += (unsigned long long)min(32, b.nrows - 32 * s) * b.wl;
+        }
+        __syncwarp();
+        res_copy_edges2d(b, En, s);
+    }
+    return core;
+}
+
+__device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S, int *take)
+{
+    __shared__ int s_flag;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Band2D b;
+    b.wl = (in.W + 31) >> 5;
+    b.npairs = (b.wl + 1) >> 1;
+    b.pp = 2 * b.npairs + 3;
+    b.r0 = it.r0;
+    b.r1 = it.r1;
+    b.a = max(0, it.r0 - it.halo);
+    const int bend = min(in.H, it.r1 + it.halo);
+    b.nrows = bend - b.a;
+    b.nstrips = (b.nrows + 31) >> 5;
+    b.zero = sm;
+    b.rows = sm + b.pp;
+    b.E = b.rows + (size_t)b.nrows * b.pp;
+    b.lastchg = reinterpret_cast<int *>(b.E + (size_t)4 * b.nstrips * b.pp);
+    const int pp = b.pp;
+
+    for (int i = threadIdx.x; i < pp; i += kResThreads) b.zero[i] = 0u;
+    for (int i = threadIdx.x; i < b.nstrips; i += kResThreads) b.lastchg[i] = kLongAgo;
+    if (threadIdx.x < 2) take[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t *g0 = in.buf[0];
+    for (int r = warp; r < b.nrows; r += kWarps) {
+        const uint32_t *grow = g0 + (size_t)(b.a + r) * in.P;
+        uint32_t *srow = b.rows + (size_t)r * pp;
+        uint32_t any = 0;
+        for (int w = lane; w < pp; w += 32) {
+            const uint32_t v = (w >= 1 && w <= b.wl) ? __ldcg(grow + (w - 1)) : 0u;
+            srow[w] = v;
+            any |= v;
+        }
+        // strips holding foreground start as "changed just before t = 0"
+        if (__any_sync(kFull, any != 0u) && lane == 0) b.lastchg[r >> 5] = -1;
+    }
+    __syncthreads();
+    for (int s = warp; s < b.nstrips; s += kWarps) res_copy_edges2d(b, b.E, s);
+    __syncthreads();
+
+    int last_any = -1;  // last subiteration with a core deletion (same in every thread)
+    int result = 0;     // 1 converged, -1 pass cap or failed wait
+    unsigned long long words = 0;
+    const int cap_t = 4 * in.pass_cap;
+    int t = 0;
+    for (;; t++) {
+        // the counter of this subiteration was cleared during the previous
+        // one; clear the next one's (nobody uses it before the barrier below)
+        if (threadIdx.x == 0) take[(t + 1) & 1] = 0;
+        uint32_t core;
+        switch (t & 3) {
+        case 0: core = res_subit2d<0>(b, t, take + (t & 1), &words); break;
+        case 1: core = res_subit2d<1>(b, t, take + (t & 1), &words); break;
+        case 2: core = res_subit2d<2>(b, t, take + (t & 1), &words); break;
+        default: core = res_subit2d<3>(b, t, take + (t & 1), &words); break;
+        }
+        if (__syncthreads_or(core != 0u)) last_any = t;
+        if (it.bands == 1) {
+            if (t - last_any >= 4) {
+                result = 1;
+                break;
+            }
+        } else if ((t & 3) == 3) {
+            // end of iteration p: trade boundary rows with the neighbouring bands
+            const int p = t >> 2;
+            const int h = it.halo;
+            uint32_t *gx = in.buf[(p + 1) & 1];  // buf[0] holds the start state other bands may still load
+            for (int k = warp; k < 2 * h; k += kWarps) {
+                const bool top = k < h;
+                if (top ? it.band == 0 : it.band + 1 == it.bands) continue;
+                const int gy = top ? b.r0 + k : b.r1 - 2 * h + k;
+                const uint32_t *srow = b.rows + (size_t)(gy - b.a) * pp;
+                uint32_t *grow = gx + (size_t)gy * in.P;
+                for (int w = lane; w < b.wl; w += 32) grow[w] = srow[w + 1];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                if (last_any >= 4 * p) atomicMax(&in.res_last, p);
+                atomicAdd(&in.res_arrive, 1);
+                int f;
+                if (!res_wait_at_least(&in.res_arrive, it.bands * (p + 1), S->timeout_ns)) {
+                    atomicOr(&S->status, kErrQueueTimeout);
+                    f = 2;
+                } else {
+                    f = ld_acquire(&in.res_last) < p ? 1 : 0;
+                }
+                s_flag = f;
+            }
+            __syncthreads();
+            const int f = s_flag;
+            if (f == 1) {
+                result = 1;
+                break;
+            }
+            if (f == 2) {
+                result = -1;
+                break;
+            }
+            // halo rows: the neighbours' boundary core rows after iteration p
+            const int ntop = b.r0 - b.a, nh = ntop + (bend - b.r1);
+            uint32_t hc = 0;
+            for (int k = warp; k < nh; k += kWarps) {
+                const int r = k < ntop ? k : (b.r1 - b.a) + (k - ntop);
+                const uint32_t *grow = gx + (size_t)(b.a + r) * in.P;
+                uint32_t *srow = b.rows + (size_t)r * pp;
+                for (int w = lane; w < b.wl; w += 32) {
+                    const uint32_t v = __ldcg(grow + w);
+                    hc |= v ^ srow[w + 1];
+                    srow[w + 1] = v;
+                }
+            }
+            if (__syncthreads_or(hc != 0u)) {
+                // the strips holding halo rows changed: mark them and refresh
+                // their edge copies for subiteration t + 1
+                uint32_t *En = b.E + ((t + 1) & 1) * (size_t)2 * b.nstrips * pp;
+                for (int s = warp; s < b.nstrips; s += kWarps) {
+                    const int ga = b.a + 32 * s, gb = b.a + min(32 * s + 32, b.nrows);
+                    if (ga >= b.r0 && gb <= b.r1) continue;
+                    if (lane == 0) b.lastchg[s] = t;
+                    res_copy_edges2d(b, En, s);
+                }
+                __syncthreads();
+            }
+        }
+        if (t >= cap_t) {
+            if (threadIdx.x == 0) atomicOr(&S->status, kErrPassLimit);
+            result = -1;
+            break;
+        }
+    }
+    // the converged core rows -> buf[0]
+    __syncthreads();
+    uint32_t *g0w = in.buf[0];
+    for (int r = b.r0 - b.a + warp; r < b.r1 - b.a; r += kWarps) {
+        const uint32_t *srow = b.rows + (size_t)r * pp;
+        uint32_t *grow = g0w + (size_t)(b.a + r) * in.P;
+        for (int w = lane; w < b.wl; w += 32) grow[w] = srow[w + 1];
+    }
+    if (lane == 0 && words) atomicAdd(&in.work_words, words / 4);  // one pass = one iteration of 4 subiterations
+    if (threadIdx.x == 0) {
+        if (it.band == 0) in.passes_run = (t + 4) / 4;
+        if (result < 0) atomicMin(&in.converged, -1);
+        atomicAdd(&in.tiles_run, 1ull);
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------ 3D ----------
+struct Vol3D {
+    uint16_t *tab;     // [nbz][nby][nbx] -> slot (0: empty)
+    int *coord;        // slot -> linear brick index
+    uint8_t *act;      // slot: active in this iteration
+    uint8_t *chg;      // slot: changed in this iteration
+    uint8_t *nxt;      // slot: active in the next iteration
+    uint16_t *list;    // active slots of this iteration
+    uint32_t *X, *Y, *U;  // slot buffers (slot 0 = the zero brick)
+    int nbx, nby, nbz, nslots;
+};
+
+// The nine row/word neighbourhood words of one plane (offset `off` within
+// the slots) from the slot bases of the rows above (u), this row (o) and
+// below (d), each for the words x-1, x, x+1.
+__device__ __forceinline__ void res_plane9(const uint32_t *IN, const int (&u)[3], const int (&o)[3],
+                                           const int (&d)[3], int off, uint32_t (&P)[9])
+{
+    const uint32_t ul = IN[u[0] + off], uc = IN[u[1] + off], ur = IN[u[2] + off];
+    const uint32_t ol = IN[o[0] + off], oc = IN[o[1] + off], orr = IN[o[2] + off];
+    const uint32_t dl = IN[d[0] + off], dc = IN[d[1] + off], dr = IN[d[2] + off];
+    P[0] = at_xm1(uc, ul); P[1] = uc; P[2] = at_xp1(uc, ur);
+    P[3] = at_xm1(oc, ol); P[4] = oc; P[5] = at_xp1(oc, orr);
+    P[6] = at_xm1(dc, dl); P[7] = dc; P[8] = at_xp1(dc, dr);
+}
+
+// Slot bases (word index of this lane's row) of the three x-neighbour bricks
+// in the z-layer dzb (-1, 0, +1) for the rows above, at and below this lane's
+// row; nb27 holds, in lane k < 27, the slot of brick offset
+// (k/9 - 1, (k/3)%3 - 1, k%3 - 1) in (z, y, x).
+__device__ __forceinline__ void res_bases3d(int nb27, int dzb, int (&u)[3], int (&o)[3], int (&d)[3])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const int so = __shfl_sync(kFull, nb27, 9 * (dzb + 1) + 3 + c);
+        const int su = __shfl_sync(kFull, nb27, 9 * (dzb + 1) + c);
+        const int sd = __shfl_sync(kFull, nb27, 9 * (dzb + 1) + 6 + c);
+        o[c] = so * kSlotWords + lane;
+        u[c] = lane == 0 ? su * kSlotWords + 31 : so * kSlotWords + lane - 1;
+        d[c] = lane == 31 ? sd * kSlotWords : so * kSlotWords + lane + 1;
+    }
+}
+
+// Subiteration J (0: pre-test union + U; 1..5: N, E, D, S, W) on brick slot s.
+template <int J>
+__device__ uint32_t res_brick3d(const Vol3D &v, int s, const uint32_t *IN, uint32_t *OUT, uint32_t *U)
+{
+    const int lane = threadIdx.x & 31;
+    const int li = v.coord[s];
+    const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
+    int nb27 = 0;
+    if (lane < 27) {
+        const int zz = bz + lane / 9 - 1, yy = by + (lane / 3) % 3 - 1, xx = bx + lane % 3 - 1;
+        if (zz >= 0 && zz < v.nbz && yy >= 0 && yy < v.nby && xx >= 0 && xx < v.nbx)
+            nb27 = v.tab[(zz * v.nby + yy) * v.nbx + xx];
+    }
+    int u[3], o[3], d[3];
+    uint32_t A[9], B[9], Cn[9];
+    res_bases3d(nb27, -1, u, o, d);
+    res_plane9(IN, u, o, d, 3 * 32, A);  // plane 4bz - 1: last plane of the brick below
+    res_bases3d(nb27, 0, u, o, d);
+    res_plane9(IN, u, o, d, 0, B);
+    const int self = s * kSlotWords + lane;
+    uint32_t chg = 0;
+#pragma unroll 1
+    for (int q = 0; q < kBZ; q++) {
+        if (q == kBZ - 1) res_bases3d(nb27, 1, u, o, d);
+        res_plane9(IN, u, o, d, ((q + 1) & 3) * 32, Cn);
+        const uint32_t val = B[4];
+        uint32_t nv = val;
+        const int widx = self + q * 32;
+        if constexpr (J == 0) {
+            uint32_t un = 0;
+            if (__any_sync(kFull, val != 0u)) {
+                uint32_t g[27];
+#pragma unroll
+                for (int i = 0; i < 9; i++) {
+                    g[i] = A[i];
+                    g[9 + i] = B[i];
+                    g[18 + i] = Cn[i];
+                }
+                const uint32_t du = rule3d<0>(g);
+                un = (du | rule3d<1>(g) | rule3d<2>(g) | rule3d<3>(g) | rule3d<4>(g) | rule3d<5>(g)) & val;
+                nv = val & ~du;
+            }
+            U[widx] = un;
+        } else {
+            const uint32_t cand = val & U[widx];
+            if (__any_sync(kFull, cand != 0u)) {
+                uint32_t g[27];
+#pragma unroll
+                for (int i = 0; i < 9; i++) {
+                    g[i] = A[i];
+                    g[9 + i] = B[i];
+                    g[18 + i] = Cn[i];
+                }
+                nv = val & ~(cand & rule3d<J>(g));
+            }
+        }
+        OUT[widx] = nv;
+        chg |= val ^ nv;
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+            A[i] = B[i];
+            B[i] = Cn[i];
+        }
+    }
+    return chg;
+}
+
+__device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S, int *take)
+{
+    (void)it;
+    __shared__ int s_cnt;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Vol3D v;
+    const int wl = (in.W + 31) >> 5;
+    v.nbx = wl;
+    v.nby = (in.H + 31) >> 5;
+    v.nbz = (in.D + kBZ - 1) / kBZ;
+    const int nb = v.nbx * v.nby * v.nbz;
+    v.tab = reinterpret_cast<uint16_t *>(smb);
+    for (int i = threadIdx.x; i < nb; i += kResThreads) v.tab[i] = 0;
+    __syncthreads();
+    // mark the non-empty bricks: one coalesced pass over the used words of
+    // the packed volume (word i of the pass = word i % wl of row i / wl)
+    const uint32_t *g0 = in.buf[0];
+    {
+        const int nw = in.D * in.H * wl;
+        for (int i = threadIdx.x; i < nw; i += kResThreads) {
+            const int r = i / wl, x = i - r * wl;
+            if (__ldcg(g0 + (size_t)r * in.P + x) != 0u) {
+                const int z = r / in.H, y = r - z * in.H;
+                v.tab[((z / kBZ) * v.nby + (y >> 5)) * v.nbx + x] = 1;
+            }
+        }
+    }
+    __syncthreads();
+    // slots in raster order of the bricks
+    const int per = (nb + kResThreads - 1) / kResThreads;
+    const int i0 = min(nb, threadIdx.x * per), i1 = min(nb, i0 + per);
+    int cnt = 0;
+    for (int i = i0; i < i1; i++) cnt += v.tab[i] != 0;
+    int total = 0;
+    const int first = res_block_exscan(cnt, &total);
+    v.nslots = total;
+    if (res_bytes3d(nb, total) > (size_t)kSmemBytes) {
+        // does not fit: the tile engine thins this volume (nothing here was written to it)
+        if (threadIdx.x == 0) in.spill = 1;
+        __syncthreads();
+        return;
+    }
+    size_t off = up16((size_t)nb * 2);
+    v.coord = reinterpret_cast<int *>(smb + off);
+    off += up16((size_t)(total + 1) * 4);
+    v.act = smb + off;
+    v.chg = v.act + (total + 1);
+    v.nxt = v.chg + (total + 1);
+    off += up16((size_t)(total + 1) * 3);
+    v.list = reinterpret_cast<uint16_t *>(smb + off);
+    off += up16((size_t)(total + 1) * 2);
+    v.X = reinterpret_cast<uint32_t *>(smb + off);
+    v.Y = v.X + (size_t)(total + 1) * kSlotWords;
+    v.U = v.Y + (size_t)(total + 1) * kSlotWords;
+    {
+        int sl = first + 1;
+        for (int i = i0; i < i1; i++)
+            if (v.tab[i]) {
+                v.tab[i] = (uint16_t)sl;
+                v.coord[sl] = i;
+                sl++;
+            }
+    }
+    for (int i = threadIdx.x; i < kSlotWords; i += kResThreads) {
+        v.X[i] = 0u;
+        v.Y[i] = 0u;
+        v.U[i] = 0u;
+    }
+    for (int i = threadIdx.x; i <= total; i += kResThreads) {
+        v.act[i] = i > 0;
+        v.chg[i] = 0;
+        v.nxt[i] = 0;
+    }
+    if (threadIdx.x < 2) take[threadIdx.x] = 0;
+    __syncthreads();
+    // gather the non-empty bricks (both state buffers)
+    for (int s = warp + 1; s <= total; s += kWarps) {
+        const int li = v.coord[s];
+        const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
+        const int y = 32 * by + lane;
+#pragma unroll
+        for (int q = 0; q < kBZ; q++) {
+            const int z = kBZ * bz + q;
+            const uint32_t w = (y < in.H && z < in.D) ? __ldcg(g0 + ((size_t)z * in.H + y) * in.P + bx) : 0u;
+            v.X[s * kSlotWords + q * 32 + lane] = w;
+            v.Y[s * kSlotWords + q * 32 + lane] = w;
+        }
+    }
+    __syncthreads();
+
+    int iter = 0, result = 0;
+    unsigned long long words = 0, bricks = 0;
+    const int cap_it = in.pass_cap / 6 + 1;
+    for (;; iter++) {
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        for (int s = threadIdx.x + 1; s <= total; s += kResThreads)
+            if (v.act[s]) v.list[atomicAdd(&s_cnt, 1)] = (uint16_t)s;
+        __syncthreads();
+        const int nact = s_cnt;
+        for (int j = 0; j < 6; j++) {
+            if (threadIdx.x == 0) take[(j + 1) & 1] = 0;
+            const uint32_t *IN = (j & 1) ? v.Y : v.X;
+            uint32_t *OUT = (j & 1) ? v.X : v.Y;
+            for (;;) {
+                const int k = res_take(take + (j & 1));
+                if (k >= nact) break;
+                const int s = v.list[k];
+                uint32_t c;
+                switch (j) {
+                case 0: c = res_brick3d<0>(v, s, IN, OUT, v.U); break;
+                case 1: c = res_brick3d<1>(v, s, IN, OUT, v.U); break;
+                case 2: c = res_brick3d<2>(v, s, IN, OUT, v.U); break;
+                case 3: c = res_brick3d<3>(v, s, IN, OUT, v.U); break;
+                case 4: c = res_brick3d<4>(v, s, IN, OUT, v.U); break;
+                default: c = res_brick3d<5>(v, s, IN, OUT, v.U); break;
+                }
+                if (lane == 0) {
+                    const int li = v.coord[s];
+                    const int by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
+                    words += (unsigned long long)min(32, in.H - 32 * by) * min(kBZ, in.D - kBZ * bz);
+                    bricks++;
+                }
+                if (__any_sync(kFull, c != 0u) && lane == 0) v.chg[s] = 1;
+            }
+            __syncthreads();
+        }
+        // next iteration's bricks: the 3x3x3 brick neighbourhoods of the changed ones
+        int any = 0;
+        for (int s = threadIdx.x + 1; s <= total; s += kResThreads) {
+            if (!v.chg[s]) continue;
+            any = 1;
+            const int li = v.coord[s];
+            const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
+            for (int dz = -1; dz <= 1; dz++) {
+                const int zz = bz + dz;
+                if (zz < 0 || zz >= v.nbz) continue;
+                for (int dy = -1; dy <= 1; dy++) {
+                    const int yy = by + dy;
+                    if (yy < 0 || yy >= v.nby) continue;
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const int xx = bx + dx;
+                        if (xx < 0 || xx >= v.nbx) continue;
+                        const int n = v.tab[(zz * v.nby + yy) * v.nbx + xx];
+                        if (n) v.nxt[n] = 1;
+                    }
+                }
+            }
+        }
+        if (!__syncthreads_or(any)) {
+            result = 1;
+            break;
+        }
+        for (int s = threadIdx.x + 1; s <= total; s += kResThreads) {
+            v.act[s] = v.nxt[s];
+            v.nxt[s] = 0;
+            v.chg[s] = 0;
+        }
+        if (iter + 1 >= cap_it) {
+            if (threadIdx.x == 0) atomicOr(&S->status, kErrPassLimit);
+            result = -1;
+            break;
+        }
+    }
+    __syncthreads();
+    // the converged state (in X after the sixth subiteration) -> buf[0]
+    uint32_t *g0w = in.buf[0];
+    for (int s = warp + 1; s <= total; s += kWarps) {
+        const int li = v.coord[s];
+        const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
+        const int y = 32 * by + lane;
+        if (y >= in.H) continue;
+#pragma unroll
+        for (int q = 0; q < kBZ; q++) {
+            const int z = kBZ * bz + q;
+            if (z < in.D) g0w[((size_t)z * in.H + y) * in.P + bx] = v.X[s * kSlotWords + q * 32 + lane];
+        }
+    }
+    if (lane == 0 && words) {
+        atomicAdd(&in.work_words, words);
+        atomicAdd(&in.tiles_run, bricks);
+    }
+    if (threadIdx.x == 0) {
+        in.passes_run = 6 * (iter + 1);
+        in.converged = result;
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------ kernels -----
+__global__ void resident_reset_kernel(Inst *insts, int n, ResSched *S, int nitems, long long timeout_ns)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Inst &in = insts[i];
+        in.res_arrive = 0;
+        in.res_last = -1;
+        in.spill = 0;
+        if (in.res) {
+            in.converged = 1;  // lowered to -1 by a band that fails
+            in.passes_run = 0;
+            in.tiles_run = 0;
+            in.work_words = 0;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S->head = 0;
+        S->nitems = nitems;
+        S->status = 0;
+        S->timeout_ns = timeout_ns;
+    }
+}
+
+__global__ void __launch_bounds__(kResThreads, 1) resident_kernel(Inst *insts, const ResItem *items, ResSched *S)
+{
+    extern __shared__ __align__(16) uint8_t res_smem[];
+    __shared__ int s_item;
+    __shared__ int s_take[2];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&S->head, 1);
+        __syncthreads();
+        const int k = s_item;
+        __syncthreads();
+        if (k >= S->nitems) break;
+        const ResItem it = items[k];
+        Inst &in = insts[it.inst];
+        if (in.dims == 2)
+            res_run2d(in, it, reinterpret_cast<uint32_t *>(res_smem), S, s_take);
+        else
+            res_run3d(in, it, res_smem, S, s_take);
+    }
+}
+
+cudaError_t res_occupancy(int *per_sm)
+{
+    cudaError_t e = cudaFuncSetAttribute(resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, resident_kernel, kResThreads, kSmemBytes);
+}
+
+cudaError_t launch_resident(int grid, Inst *d_insts, int ninst, const ResItem *d_items, int nitems,
+                            ResSched *d_rs, long long timeout_ns, cudaStream_t st)
+{
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaError_t e = cudaFuncSetAttribute(resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        if (e != cudaSuccess) return e;
+        attr_done = true;
+    }
+    resident_reset_kernel<<<std::max(1, std::min(64, (ninst + 255) / 256)), 256, 0, st>>>(d_insts, ninst, d_rs, nitems,
+                                                                                       timeout_ns);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || nitems == 0) return e;
+    // cooperative: all CTAs are resident at once, which the bands of an image
+    // (waiting for one another) rely on
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kResThreads);
+    cfg.dynamicSmemBytes = kSmemBytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, resident_kernel, d_insts, d_items, d_rs);
+}
+
+}  // namespace bgt

@@ -243,6 +243,9 @@ int setup_lane(bgt_server *S, int li, int dims, int priority, int nslots, int ma
         if ((rc = bgt_batch_create(s.ctx, &s.b)) != BGT_OK) return rc;
         if ((rc = bgt_batch_reserve(s.b, pool_bytes)) != BGT_OK) return rc;
         bgt_batch_set_grid(s.b, grid_cap);
+        // tile rings: the lanes share the SMs with one another, which the
+        // resident kernel (one 225 KB CTA on every SM at once) cannot
+        bgt_batch_set_engine(s.b, 1);
         e = cudaMalloc(&s.d_io, io_cap);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(serving staging)");
         s.io_cap = io_cap;

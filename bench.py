@@ -52,7 +52,6 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="bgt", choices=["bgt", "reference"])
     p.add_argument("--seed", type=int, default=3)
-    p.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     p.add_argument("--n2d", type=int, default=512, help="2D instances per GPU (smaller only for profiling)")
     p.add_argument("--n3d", type=int, default=32, help="3D instances per GPU (smaller only for profiling)")
     p.add_argument("--no-plain", action="store_true")
@@ -63,6 +62,8 @@ def parse():
                    help="device buffer sets used in turn by consecutive host-to-host steps")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-centerline", action="store_true", help="skip the CenterlineExtraction timing block")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the single-instance legs (512^2 strokes, 4096^2 vessels, 256^3 trees)")
     p.add_argument("--serve-seconds", type=float, default=4.0, help="measured seconds of the serving run")
     return p.parse_args()
 
@@ -154,9 +155,9 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the engine kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "engine_kernel_mixed_batch.md")
+def ncu_traffic(kernel: str = "engine_kernel"):
+    """Per-launch DRAM bytes of `kernel` on the mixed batch from its committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_mixed_batch.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -172,26 +173,21 @@ def workload(seed: int, n2d: int = 512, n3d: int = 32):
     return imgs + vols
 
 
-def cpu_baseline(items, budget_s: float) -> dict:
-    """The oracle's OpenMP thinning on this host, on the first instances of
-    the batch until the time budget is spent."""
+def oracle_outputs(items):
+    """The oracle's thinning of every instance (OpenMP over this host's
+    cores), timed: the parity reference of the whole batch and the CPU
+    baseline in one pass."""
     from oracle import pyoracle as po
     cores = host_cores()
+    outs = []
     t0 = time.perf_counter()
-    vox = 0
-    n = 0
     for it in items:
-        if it.ndim == 2:
-            po.thin2d(it, cores)
-        else:
-            po.thin3d(it, cores)
-        vox += it.size
-        n += 1
-        if time.perf_counter() - t0 > budget_s:
-            break
+        outs.append(po.thin2d(it, cores)[0] if it.ndim == 2 else po.thin3d(it, cores)[0])
     dt = time.perf_counter() - t0
-    return {"value": vox / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {n} of {len(items)} instances ({vox / 1e6:.1f} Mvoxel), oracle OpenMP thinning"}
+    vox = sum(it.size for it in items)
+    base = {"value": vox / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"all {len(items)} instances ({vox / 1e6:.1f} Mvoxel), oracle OpenMP thinning"}
+    return outs, base
 
 
 def run_bgt(args, rank, world, local):
@@ -245,19 +241,18 @@ def run_bgt(args, rank, world, local):
             step()
     torch.cuda.synchronize()
 
-    # bit-exactness spot check of a few instances against the oracle
-    from oracle import pyoracle as po
+    # bit-exactness of every instance of the timed batch against the oracle
     out_np = dev_out.cpu().numpy()
-    rng = np.random.default_rng(rank)
-    small = [k for k, it in enumerate(items) if it.size <= 300_000]
+    want_all, cpu_base = oracle_outputs(items)
     checked = 0
-    for k in rng.choice(small, size=min(6, len(small)), replace=False):
-        it = items[k]
-        want = po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
+    for k, (it, want) in enumerate(zip(items, want_all)):
         got = out_np[offs[k]:offs[k] + it.size].reshape(it.shape)
         if not np.array_equal(got, want):
-            raise SystemExit(f"bench parity check failed on instance {k} shape {it.shape}")
+            raise SystemExit(f"bench parity check failed on instance {k} shape {it.shape}: "
+                             f"{int((got != want).sum())} voxels differ")
         checked += 1
+    del want_all
+    plans = [b.plan(i) for i in ids]
 
     gpu_uuid = None
     try:
@@ -287,14 +282,17 @@ def run_bgt(args, rank, world, local):
     ms = e0.elapsed_time(e1) / args.steps
 
     # engine kernel alone: stage events recorded by the library on the same stream
-    eng_ms, pack_ms, unpack_ms = [], [], []
+    eng_ms, pack_ms, unpack_ms, res_ms, ring_ms = [], [], [], [], []
     for _ in range(max(3, args.steps // 2)):
         with torch.cuda.stream(stream):
             step()
         p, e, u = b.stage_ms()
+        r, g = b.engine_ms()
         eng_ms.append(e)
         pack_ms.append(p)
         unpack_ms.append(u)
+        res_ms.append(r)
+        ring_ms.append(g)
     tiles, words = b.work()
 
     # end to end: pinned host -> device, thin, device -> pinned host
@@ -377,8 +375,16 @@ def run_bgt(args, rank, world, local):
         return None
     peak, peak_kind = measured_peaks()
     eng = statistics.median(eng_ms)
+    res, ring = statistics.median(res_ms), statistics.median(ring_ms)
+    n_res = sum(1 for r, _ in plans if r)
+    # the dominant kernel: the resident kernel when it takes the batch, else the tile-ring engine
+    kernel, kms = ("resident_kernel", res) if res >= ring else ("engine_kernel", ring)
     alg_bytes = words * 8.0  # one 4-byte read + one 4-byte write per packed core word per pass
-    achieved = alg_bytes / (eng * 1e-3) / 1e9
+    achieved = alg_bytes / (kms * 1e-3) / 1e9
+    # kernels per step: batch pack, scheduler reset, resident reset, resident kernel, the
+    # tile-ring seed + engine (when some instance may use them), batch unpack
+    any_ring = n_res < len(items) or any(it.ndim == 3 for it in items)
+    launches_per_step = 4 + (1 if n_res else 0) + (2 if any_ring else 0)
     n2 = sum(1 for it in items if it.ndim == 2)
     line = {
         "metric": METRIC,
@@ -406,11 +412,13 @@ def run_bgt(args, rank, world, local):
                         f"buffer sets used in turn by consecutive steps (PipelinedBatch)",
                 "serial_value": units / (e2e_serial_ms * 1e-3) / 1e6},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,
-                     "kernel": "engine_kernel", "launch_ms": eng,
-                     "algorithmic_bytes_per_launch": alg_bytes, "tile_passes": tiles},
-        "stage_ms": {"pack": statistics.median(pack_ms), "engine": eng, "unpack": statistics.median(unpack_ms)},
-        "gpu_launches": 5 * args.steps,
+                     "frac": achieved / peak, "traffic": ncu_traffic(kernel), "peak_kind": peak_kind,
+                     "kernel": kernel, "launch_ms": kms,
+                     "algorithmic_bytes_per_launch": alg_bytes, "work_units": tiles},
+        "stage_ms": {"pack": statistics.median(pack_ms), "engine": eng, "resident_kernel": res,
+                     "tile_rings": ring, "unpack": statistics.median(unpack_ms)},
+        "instances_resident": n_res,
+        "gpu_launches": launches_per_step * args.steps,
         "parity_checked_instances": checked,
         "clocks": clk,
     }
@@ -420,7 +428,7 @@ def run_bgt(args, rank, world, local):
     b.close()
     ctx.close()
     if world == 1:
-        line["cpu_baseline"] = cpu_baseline(items, args.cpu_seconds)
+        line["cpu_baseline"] = cpu_base
         if not args.no_serve:
             from begputhinning_b200.serve import run_workload
             s = run_workload(duration_s=args.serve_seconds, device=local)
@@ -437,7 +445,116 @@ def run_bgt(args, rank, world, local):
             }
         if not args.no_centerline:
             line["centerline"] = centerline_block()
+        if not args.no_configs:
+            line["configs"] = config_legs(local, peak, peak_kind)
     return line
+
+
+def config_legs(local: int, peak: float, peak_kind: str, reps: int = 10) -> dict:
+    """The single-instance workloads at their named sizes: 512x512 Bezier
+    strokes, 4096x4096 vessel trees with salt and holes, 256^3 tubular trees
+    with ellipsoids.  Per workload, thinning and segment extraction are
+    timed separately: thinning device-resident (pack + engine + unpack of a
+    one-instance batch, CUDA events on its stream, graph replay) and end to
+    end through the host API (Thinning2D/Thinning3D: host buffers, copies
+    included); segments by the device ExtractSegmentsV on the thinned image.
+    Beside them the reference's own CPU code on the same input: its rule
+    functions run globally with OpenMP on every host core (oracle/_ref), and
+    its single-threaded ExtractSegmentsV; outputs are compared."""
+    import numpy as np
+    import torch
+
+    import begputhinning_b200 as bgt
+    from begputhinning_b200 import synth
+    from oracle import pyoracle as po
+    cores = host_cores()
+    cases = [("strokes_512x512", synth.frame512(0)),
+             ("vessels_4096x4096", synth.vessels4096(1)),
+             ("trees_256x256x256", synth.trees256(2))]
+    dev = torch.device("cuda", local)
+    ctx = bgt.Context(local)
+    stream = torch.cuda.Stream(dev)
+    ctx.set_stream(stream)
+    out = {}
+    for name, data in cases:
+        e = {"shape": list(data.shape), "voxels": int(data.size), "foreground": float((data != 0).mean())}
+        d_in = torch.from_numpy(data).to(dev)
+        d_out = torch.empty_like(d_in)
+        b = bgt.Batch(ctx)
+        i = b.add(data.shape)
+        b.finalize()
+        b.set_io(i, d_in, d_out)
+        resident, bands = b.plan(i)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                b.run(graph=True, sync=False)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(reps):
+                b.run(graph=True, sync=False)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        pk, en, un = b.stage_ms()
+        rk, rg = b.engine_ms()
+        _, words = b.work()
+        st = b.stats(i)
+        thinned = d_out.cpu().numpy()
+        kms = rk if rk >= rg else rg
+        achieved = words * 8.0 / (kms * 1e-3) / 1e9
+        e["thinning"] = {
+            "ms": ms, "mvoxel_per_s": data.size / ms / 1e3, "stage_ms": {"pack": pk, "engine": en, "unpack": un},
+            "engine_kernels_ms": {"resident_kernel": rk, "tile_rings": rg}, "iterations": st["passes"],
+            "resident": resident, "bands": bands,
+            "roofline": {"bound": "hbm", "kernel": "resident_kernel" if rk >= rg else "engine_kernel",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": words * 8.0}}
+        b.close()
+        thin_api = bgt.Thinning2D if data.ndim == 2 else bgt.Thinning3D
+        thin_api(data, ctx)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            api_out = thin_api(data, ctx)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        e2e = statistics.median(ts)
+        e["thinning"]["e2e"] = {"ms": e2e, "mvoxel_per_s": data.size / e2e / 1e3,
+                                "path": "Thinning2D/Thinning3D C ABI: host buffer in, host buffer out"}
+        segs = bgt.ExtractSegmentsV(d_out, ctx)
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            segs = bgt.ExtractSegmentsV(d_out, ctx)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        e["segments"] = {"ms": statistics.median(ts), "segments": int(segs.nseg),
+                         "path": "device ExtractSegmentsV on the thinned image in device memory, "
+                                 "segment arrays copied to the host"}
+        which = "2d" if data.ndim == 2 else "3d"
+        if po.have_ref(which):
+            t0 = time.perf_counter()
+            ref_thin = po.ref_thin2d(data) if data.ndim == 2 else po.ref_thin3d(data)
+            ref_ms = (time.perf_counter() - t0) * 1e3
+            t0 = time.perf_counter()
+            ref_segs = po.ref_segments2d(ref_thin) if data.ndim == 2 else po.ref_segments3d(ref_thin)
+            seg_ms = (time.perf_counter() - t0) * 1e3
+            e["reference_cpu"] = {
+                "thinning_ms": ref_ms, "thinning_mvoxel_per_s": data.size / ref_ms / 1e3, "thinning_cores": cores,
+                "segments_ms": seg_ms, "segments_threads": 1,
+                "kind": "reference (its rule functions with a global synchronous OpenMP driver; its ExtractSegmentsV)"}
+            e["identical_to_reference"] = {
+                "thinning": bool(np.array_equal(thinned, ref_thin) and np.array_equal(api_out, ref_thin)),
+                "segments": segs.as_lists() == ref_segs.as_lists()}
+            e["speedup_vs_reference_cpu"] = {"thinning_e2e": ref_ms / e2e, "segments": seg_ms / e["segments"]["ms"]}
+        if name.startswith("vessels"):
+            e["reference_gpu"] = ("not run: the reference's Thinning2D divides by zero on the host for widths "
+                                  "2049-4096 (2D/LibThinning2D.cu:66)")
+        out[name] = e
+    ctx.close()
+    return out
 
 
 def centerline_block(calls: int = 10) -> dict:

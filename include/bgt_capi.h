@@ -165,8 +165,20 @@ int bgt_batch_device_bytes(bgt_batch *b, size_t *bytes);
  * 4 bytes each is the algorithmic traffic of a word-pass) */
 int bgt_batch_work(bgt_batch *b, unsigned long long *tiles, unsigned long long *words);
 /* device milliseconds of the last engine run's stages (CUDA events on the
- * batch's stream): pack, engine (the persistent thinning kernel), unpack */
+ * batch's stream): pack, engine (the thinning kernels), unpack */
 int bgt_batch_stage_ms(bgt_batch *b, float *pack_ms, float *engine_ms, float *unpack_ms);
+/* The engine stage split: the resident kernel (instances thinned inside
+ * one CTA's shared memory, large images as bands of CTAs) and the tile-ring
+ * engine after it (instances the resident kernel does not take, volumes
+ * whose non-empty bricks did not fit). */
+int bgt_batch_engine_ms(bgt_batch *b, float *resident_ms, float *rings_ms);
+/* Engine choice for the next finalize: 0 = resident kernel wherever an
+ * instance fits (default), 1 = tile rings only.  Instances added with an
+ * explicit configuration (cfg >= 0) always use the tile rings. */
+int bgt_batch_set_engine(bgt_batch *b, int mode);
+/* Plan of instance id after finalize: *resident = 1 when the resident
+ * kernel takes it, *bands = the CTAs a 2D image is cut into (0 for rings). */
+int bgt_batch_plan(bgt_batch *b, int id, int *resident, int *bands);
 
 /* ---- serving -------------------------------------------------------------
  * A request loop over the batch engine.  Requests (2D frames: depth 1; 3D
