@@ -22,7 +22,7 @@ EXPORTS = [
     "bgt_batch_engine_ms", "bgt_batch_set_engine", "bgt_batch_plan",
     "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe", "bgt_rule_table",
     "bgt_server_create", "bgt_server_submit", "bgt_server_poll", "bgt_server_drain", "bgt_server_stats",
-    "bgt_server_reset_stats", "bgt_server_destroy",
+    "bgt_server_reset_stats", "bgt_server_destroy", "bgt_server_memory",
 ]
 
 
@@ -95,6 +95,7 @@ def _declare(L):
         "bgt_server_stats": [vp, I, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                              C.POINTER(C.c_ulonglong)],
         "bgt_server_reset_stats": [vp],
+        "bgt_server_memory": [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_ulonglong)],
         "bgt_server_destroy": [vp],
     }
     for name, args in sig.items():

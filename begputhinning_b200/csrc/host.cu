@@ -182,8 +182,20 @@ static void batch_free_device(bgt_batch *b)
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;
     b->graph_valid = false;
-    if (b->pool) cudaFree(b->pool);
+    if (b->pool && !b->external) cudaFree(b->pool);
     b->pool = nullptr;
+}
+
+int bgt::batch_use_pool(bgt_batch *b, void *pool, size_t bytes)
+{
+    if (!b || !pool) return fail(BGT_ERR_ARG, "null argument");
+    if (b->finalized) return fail(BGT_ERR_STATE, "set the pool before finalize");
+    if (b->pool && !b->external) return fail(BGT_ERR_STATE, "the batch already owns a pool");
+    b->pool = pool;
+    b->pool_bytes = bytes;
+    b->reserved = true;
+    b->external = true;
+    return BGT_OK;
 }
 
 extern "C" int bgt_batch_destroy(bgt_batch *b)
@@ -294,6 +306,99 @@ static void plan_resident(bgt_batch *b)
         if (!b->h[i].res) b->any_ring = true;
 }
 
+// Tile geometry and limits of one instance (no device memory yet).
+static void init_inst(BatchItem &it, Inst &in)
+{
+    if (it.cfg < 0) it.cfg = tuned_cfg(it.dims, it.W, it.H, it.D);
+    const CfgInfo &c = *cfg_info(it.cfg);
+    memset(&in, 0, sizeof(in));
+    in.dims = it.dims;
+    in.W = it.W;
+    in.H = it.H;
+    in.D = it.D;
+    in.P = (int)align_up((size_t)(it.W + 31) / 32, 4);
+    in.cfg = it.cfg;
+    in.TW = c.TW;
+    in.TH = c.TH;
+    in.TZ = c.TZc;
+    in.k = c.k;
+    in.window = std::max(1, (4 + c.k - 1) / c.k);
+    const int wwords = (it.W + 31) / 32;
+    in.tiles_x = (wwords + c.TW - 1) / c.TW;
+    in.tiles_y = (it.H + c.TH - 1) / c.TH;
+    in.tiles_z = (it.D + c.TZc - 1) / c.TZc;
+    in.ntiles = in.tiles_x * in.tiles_y * in.tiles_z;
+    const int maxdim = std::max(it.W, std::max(it.H, it.D));
+    const int passes_per_iter = it.dims == 3 ? 6 : std::max(1, 4 / c.k);
+    in.pass_cap = (maxdim + 16) * passes_per_iter + 64;
+    // 3D instances carry the longest chains of dependent passes (six
+    // passes per iteration): their waves go to the ring served first
+    in.prio = it.dims == 3 ? 0 : 1;
+}
+
+// Offsets of everything a batch keeps in its device pool.
+struct InstOffs {
+    size_t b0, b1, uni, lc, act, list;
+};
+struct PoolLayout {
+    std::vector<InstOffs> offs;
+    size_t off_lc = 0, lc_bytes = 0, off_io = 0, off_sched = 0, off_seq = 0, off_item = 0, off_inst = 0,
+           off_tmap = 0, off_flag = 0, off_res = 0, off_rs = 0, total = 0;
+    unsigned cap = 0;
+};
+
+static PoolLayout layout_pool(const std::vector<Inst> &h, size_t n_res_items)
+{
+    PoolLayout L;
+    const int N = (int)h.size();
+    L.offs.resize(N);
+    size_t off = 0, total_tiles = 0;
+    for (int i = 0; i < N; i++) {
+        const Inst &in = h[i];
+        const size_t words = (size_t)in.P * in.H * in.D;
+        InstOffs &o = L.offs[i];
+        o.b0 = off; off = align_up(off + words * 4, 256);
+        o.b1 = off; off = align_up(off + words * 4, 256);
+        o.uni = 0;
+        if (in.dims == 3) { o.uni = off; off = align_up(off + words * 4, 256); }
+        o.act = off; off = align_up(off + (size_t)in.ntiles, 256);
+        o.list = off; off = align_up(off + (size_t)in.ntiles * 4, 256);
+        total_tiles += in.ntiles;
+    }
+    // all per-tile "last change" arrays in one block (one memset per run)
+    L.off_lc = off;
+    for (int i = 0; i < N; i++) {
+        L.offs[i].lc = off;
+        off += (size_t)h[i].ntiles * 4;
+    }
+    L.lc_bytes = off - L.off_lc;
+    off = align_up(off, 256);
+    L.off_io = off; off = align_up(off + (size_t)N * sizeof(IODesc), 256);
+    // scheduler + ring + instance table + tensor maps + flags
+    L.cap = (unsigned)(total_tiles + 1024);
+    L.off_sched = off; off = align_up(off + sizeof(Sched), 256);
+    L.off_seq = off; off = align_up(off + (size_t)L.cap * 4 * 2, 256);
+    L.off_item = off; off = align_up(off + (size_t)L.cap * sizeof(int4) * 2, 256);
+    L.off_inst = off; off = align_up(off + (size_t)N * sizeof(Inst), 256);
+    L.off_tmap = off; off = align_up(off + (size_t)N * kMapsPerInst * sizeof(CUtensorMap), 256);
+    L.off_flag = off; off = align_up(off + 64, 256);
+    // resident engine: item list + its scheduler
+    L.off_res = off; off = align_up(off + std::max<size_t>(1, n_res_items) * sizeof(ResItem), 256);
+    L.off_rs = off; off = align_up(off + sizeof(ResSched), 256);
+    L.total = off;
+    return L;
+}
+
+// Device pool bytes a tile-ring batch of these shapes needs (the serving
+// runtime sizes its admissions with it).
+size_t bgt::batch_pool_bytes(const std::vector<BatchItem> &items)
+{
+    std::vector<BatchItem> its = items;
+    std::vector<Inst> h(its.size());
+    for (size_t i = 0; i < its.size(); i++) init_inst(its[i], h[i]);
+    return layout_pool(h, 0).total;
+}
+
 extern "C" int bgt_batch_finalize(bgt_batch *b)
 {
     if (!b) return fail(BGT_ERR_ARG, "null batch");
@@ -302,67 +407,11 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     cudaSetDevice(b->ctx->device);
     const int N = (int)b->items.size();
     b->h.assign(N, Inst());
-    size_t off = 0;
-    size_t total_tiles = 0;
     int max_smem = 0;
-    struct Offs { size_t b0, b1, uni, lc, act, list; };
-    std::vector<Offs> offs(N);
     for (int i = 0; i < N; i++) {
-        BatchItem &it = b->items[i];
-        if (it.cfg < 0) it.cfg = tuned_cfg(it.dims, it.W, it.H, it.D);
-        const CfgInfo &c = *cfg_info(it.cfg);
-        Inst &in = b->h[i];
-        memset(&in, 0, sizeof(in));
-        in.dims = it.dims;
-        in.W = it.W;
-        in.H = it.H;
-        in.D = it.D;
-        in.P = (int)align_up((size_t)(it.W + 31) / 32, 4);
-        in.cfg = it.cfg;
-        in.TW = c.TW;
-        in.TH = c.TH;
-        in.TZ = c.TZc;
-        in.k = c.k;
-        in.window = std::max(1, (4 + c.k - 1) / c.k);
-        const int wwords = (it.W + 31) / 32;
-        in.tiles_x = (wwords + c.TW - 1) / c.TW;
-        in.tiles_y = (it.H + c.TH - 1) / c.TH;
-        in.tiles_z = (it.D + c.TZc - 1) / c.TZc;
-        in.ntiles = in.tiles_x * in.tiles_y * in.tiles_z;
-        const int maxdim = std::max(it.W, std::max(it.H, it.D));
-        const int passes_per_iter = it.dims == 3 ? 6 : std::max(1, 4 / c.k);
-        in.pass_cap = (maxdim + 16) * passes_per_iter + 64;
-        // 3D instances carry the longest chains of dependent passes (six
-        // passes per iteration): their waves go to the ring served first
-        in.prio = it.dims == 3 ? 0 : 1;
-        const size_t words = (size_t)in.P * it.H * it.D;
-        Offs &o = offs[i];
-        o.b0 = off; off = align_up(off + words * 4, 256);
-        o.b1 = off; off = align_up(off + words * 4, 256);
-        if (it.dims == 3) { o.uni = off; off = align_up(off + words * 4, 256); }
-        o.act = off; off = align_up(off + (size_t)in.ntiles, 256);
-        o.list = off; off = align_up(off + (size_t)in.ntiles * 4, 256);
-        total_tiles += in.ntiles;
-        max_smem = std::max(max_smem, c.smem);
+        init_inst(b->items[i], b->h[i]);
+        max_smem = std::max(max_smem, cfg_info(b->items[i].cfg)->smem);
     }
-    // all per-tile "last change" arrays in one block (one memset per run)
-    const size_t off_lc = off;
-    for (int i = 0; i < N; i++) {
-        offs[i].lc = off;
-        off += (size_t)b->h[i].ntiles * 4;
-    }
-    b->lc_bytes = off - off_lc;
-    off = align_up(off, 256);
-    const size_t off_io = off; off = align_up(off + (size_t)N * sizeof(IODesc), 256);
-    // scheduler + ring + instance table + tensor maps + flags
-    const unsigned cap = (unsigned)(total_tiles + 1024);
-    const size_t off_sched = off; off = align_up(off + sizeof(Sched), 256);
-    const size_t off_seq = off; off = align_up(off + (size_t)cap * 4 * 2, 256);
-    const size_t off_item = off; off = align_up(off + (size_t)cap * sizeof(int4) * 2, 256);
-    const size_t off_inst = off; off = align_up(off + (size_t)N * sizeof(Inst), 256);
-    const size_t off_tmap = off; off = align_up(off + (size_t)N * kMapsPerInst * sizeof(CUtensorMap), 256);
-    const size_t off_flag = off; off = align_up(off + 64, 256);
-    // resident engine: item list (at most one band per row of every image) + its scheduler
     {
         int per_sm = 0;
         if (res_occupancy(&per_sm) == cudaSuccess && per_sm > 0) b->res_grid = b->ctx->sms * per_sm;
@@ -370,8 +419,13 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
         if (b->grid_cap > 0) b->res_grid = std::min(b->res_grid, b->grid_cap);
     }
     plan_resident(b);
-    const size_t off_res = off; off = align_up(off + std::max<size_t>(1, b->res_items.size()) * sizeof(ResItem), 256);
-    const size_t off_rs = off; off = align_up(off + sizeof(ResSched), 256);
+    const PoolLayout L = layout_pool(b->h, b->res_items.size());
+    const std::vector<InstOffs> &offs = L.offs;
+    const size_t off = L.total, off_lc = L.off_lc, off_io = L.off_io, off_sched = L.off_sched,
+                 off_seq = L.off_seq, off_item = L.off_item, off_inst = L.off_inst, off_tmap = L.off_tmap,
+                 off_flag = L.off_flag, off_res = L.off_res, off_rs = L.off_rs;
+    const unsigned cap = L.cap;
+    b->lc_bytes = L.lc_bytes;
     cudaError_t e;
     if (b->reserved) {
         // a reserved pool is re-laid-out for every set of instances, never reallocated
@@ -399,7 +453,7 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     maps.assign((size_t)N * kMapsPerInst, CUtensorMap());
     for (int i = 0; i < N; i++) {
         Inst &in = b->h[i];
-        const Offs &o = offs[i];
+        const InstOffs &o = offs[i];
         in.buf[0] = (uint32_t *)(P + o.b0);
         in.buf[1] = (uint32_t *)(P + o.b1);
         in.uni = in.dims == 3 ? (uint32_t *)(P + o.uni) : nullptr;

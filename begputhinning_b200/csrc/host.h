@@ -48,6 +48,10 @@ int ctx_scratch(bgt_ctx *c, int slot, size_t bytes, void **out);
 int single_batch(bgt_ctx *c, int dims, int W, int H, int D, bgt_batch **out);
 int batch_check(bgt_batch *b);
 int batch_set_input_extent(bgt_batch *b, int id, int inW, int inH, int inD);
+size_t batch_pool_bytes(const std::vector<BatchItem> &items);
+// Lay a batch out in caller-provided device memory (the serving runtime's
+// arena) from the next finalize on; the memory is not freed by the batch.
+int batch_use_pool(bgt_batch *b, void *pool, size_t bytes);
 
 // Segment list on the host (malloc'ed arrays), in the reference's emission order.
 struct HostSegs {
@@ -94,7 +98,8 @@ struct bgt_batch {
     void *pool = nullptr;
     size_t pool_bytes = 0;
     size_t used_bytes = 0;
-    bool reserved = false;              // pool pre-allocated by bgt_batch_reserve
+    bool reserved = false;              // pool pre-allocated by bgt_batch_reserve (or external)
+    bool external = false;              // pool owned by the caller (batch_use_pool), never freed here
     int grid_cap = 0;                   // engine CTA cap (0: full device)
     std::vector<CUtensorMap> maps;      // host copies of uploaded tables (kept
     std::vector<bgt::IODesc> io_host;   // alive for stream-ordered uploads)

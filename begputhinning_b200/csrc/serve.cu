@@ -6,17 +6,23 @@
 // granularity); a completion thread stamps each request's latency when its
 // output is back in host memory.
 //
-// Lanes: 0 = 2D frames on a high-priority stream, 1 = 3D volumes on a
-// low-priority stream.  Each lane owns a few slots; a slot is a reserved
-// batch pool plus resident device staging for inputs and outputs, so the
-// loop allocates nothing per request.  All slot memory together stays
-// within the HBM budget given at creation; a request is admitted only when a
-// slot of its lane is free and has room for it.
+// Lanes: 0 = 2D frames on high-priority streams, 1 = 3D volumes on
+// low-priority streams.  Each lane has a few slots (a stream, a context and
+// a batch: launches of different slots overlap on the device).  Device
+// memory is one arena of the HBM budget, allocated at creation and resident:
+// every launch takes one block of it (staging for its requests' inputs and
+// outputs plus its batch's pool, sized from the requests' shapes) and
+// returns it when its outputs are back in host memory.  A request is
+// admitted when a slot of its lane is free and the arena has room for the
+// launch grown by it; until then it waits.  The lanes share the arena and
+// borrow each other's idle memory, except that volumes leave a guard large
+// enough for one launch of frames.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -44,14 +50,13 @@ struct Req {
     int status = 0;
 };
 
-// One slot = one stream (of the lane's priority), a context bound to it, a
-// reserved batch and resident staging: slots of a lane overlap on the device.
+// One slot = one stream (of the lane's priority), a context bound to it and
+// a batch laid out in the launch's arena block: slots overlap on the device.
 struct Slot {
     bgt_ctx *ctx = nullptr;
     cudaStream_t stream = nullptr;
     bgt_batch *b = nullptr;
-    char *d_io = nullptr;  // inputs, then outputs
-    size_t io_cap = 0;
+    size_t blk_off = 0, blk_len = 0;  // arena block of the launch in flight (staging, then pool)
     cudaEvent_t done = nullptr;
     bool busy = false;      // holds admitted requests
     bool launched = false;  // its work (ending with `done`) is enqueued
@@ -64,18 +69,85 @@ struct Lane {
     std::vector<Slot> slots;
     std::deque<Req *> pending;
     int max_batch = 16;
-    size_t pool_bytes = 0;
+    size_t cap = 0;   // arena bytes the lane may hold at once
+    size_t used = 0;  // arena bytes its launches hold now
     std::vector<double> lat_ms;
     unsigned long long done = 0;
     double voxels = 0;
     double t_first = 0, t_last = 0;
 };
 
+// First-fit allocator over the arena, coalescing on release.
+struct Arena {
+    char *base = nullptr;
+    size_t size = 0, used = 0;
+    std::map<size_t, size_t> free;  // offset -> length
+    size_t largest() const
+    {
+        size_t m = 0;
+        for (auto &kv : free) m = std::max(m, kv.second);
+        return m;
+    }
+    bool alloc(size_t n, size_t *off)
+    {
+        for (auto it = free.begin(); it != free.end(); ++it) {
+            if (it->second < n) continue;
+            *off = it->first;
+            const size_t rest = it->second - n, at = it->first + n;
+            free.erase(it);
+            if (rest) free[at] = rest;
+            used += n;
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t n)
+    {
+        used -= n;
+        auto it = free.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free.erase(nx);
+        }
+        if (it != free.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free.erase(it);
+            }
+        }
+    }
+};
+
+size_t up256(size_t v) { return (v + 255) / 256 * 256; }
+
+// Arena bytes of one launch of these requests: staging (inputs and
+// outputs) plus the batch pool their shapes need.
+size_t launch_bytes(const std::vector<Req *> &reqs, int cfg)
+{
+    size_t staging = 0;
+    std::vector<BatchItem> items;
+    for (const Req *r : reqs) {
+        staging += 2 * up256(r->bytes);
+        BatchItem it;
+        it.dims = r->dims;
+        it.W = r->w;
+        it.H = r->h;
+        it.D = r->d;
+        it.cfg = cfg;
+        it.auto_cfg = cfg < 0;
+        items.push_back(it);
+    }
+    return staging + up256(batch_pool_bytes(items)) + 256;
+}
+
 }  // namespace
 
 struct bgt_server {
     int device = 0;
-    size_t budget = 0, reserved = 0;
+    size_t budget = 0;
+    Arena arena;
     std::mutex mu;
     std::condition_variable cv;
     Lane lane[2];
@@ -90,24 +162,28 @@ struct bgt_server {
 
 namespace {
 
-// Launch the requests now held by `s` (called without the server lock).
+// Launch the requests now held by `s` in its arena block (called without
+// the server lock).
 int launch_slot(bgt_server *S, Slot &s)
 {
     bgt_batch *b = s.b;
     int rc = bgt_batch_reset(b);
+    char *blk = S->arena.base + s.blk_off;
     size_t off = 0;
     std::vector<size_t> in_off(s.reqs.size()), out_off(s.reqs.size());
     for (size_t i = 0; i < s.reqs.size(); i++) {
         in_off[i] = off;
-        off += (s.reqs[i]->bytes + 255) / 256 * 256;
+        off += up256(s.reqs[i]->bytes);
     }
     for (size_t i = 0; i < s.reqs.size(); i++) {
         out_off[i] = off;
-        off += (s.reqs[i]->bytes + 255) / 256 * 256;
+        off += up256(s.reqs[i]->bytes);
     }
+    if (rc == BGT_OK) rc = batch_use_pool(b, blk + off, s.blk_len - off);
+    if (rc != BGT_OK) return rc;
     cudaError_t e = cudaSuccess;
     for (size_t i = 0; i < s.reqs.size() && e == cudaSuccess; i++)
-        e = cudaMemcpyAsync(s.d_io + in_off[i], s.reqs[i]->host_in, s.reqs[i]->bytes, cudaMemcpyHostToDevice,
+        e = cudaMemcpyAsync(blk + in_off[i], s.reqs[i]->host_in, s.reqs[i]->bytes, cudaMemcpyHostToDevice,
                             s.stream);
     if (e != cudaSuccess) return cuda_fail(e, "serve H2D");
     for (size_t i = 0; i < s.reqs.size() && rc == BGT_OK; i++) {
@@ -117,11 +193,11 @@ int launch_slot(bgt_server *S, Slot &s)
     }
     if (rc == BGT_OK) rc = bgt_batch_finalize(b);
     for (size_t i = 0; i < s.reqs.size() && rc == BGT_OK; i++)
-        rc = bgt_batch_set_io(b, (int)i, s.reqs[i]->dtype, s.d_io + in_off[i], s.d_io + out_off[i]);
+        rc = bgt_batch_set_io(b, (int)i, s.reqs[i]->dtype, blk + in_off[i], blk + out_off[i]);
     if (rc == BGT_OK) rc = bgt_batch_run(b, 0, 0);
     if (rc != BGT_OK) return rc;
     for (size_t i = 0; i < s.reqs.size() && e == cudaSuccess; i++)
-        e = cudaMemcpyAsync(s.reqs[i]->host_out, s.d_io + out_off[i], s.reqs[i]->bytes, cudaMemcpyDeviceToHost,
+        e = cudaMemcpyAsync(s.reqs[i]->host_out, blk + out_off[i], s.reqs[i]->bytes, cudaMemcpyDeviceToHost,
                             s.stream);
     if (e == cudaSuccess) e = cudaEventRecord(s.done, s.stream);
     if (e != cudaSuccess) return cuda_fail(e, "serve D2H");
@@ -139,17 +215,28 @@ void dispatcher_loop(bgt_server *S)
             Lane &L = S->lane[li];
             for (Slot &s : L.slots) {
                 if (s.busy || L.pending.empty()) continue;
-                // admit from the front while the slot has room
-                size_t used = 0;
+                // admit from the front while the lane's share and the arena
+                // have room for the launch grown by the next request
+                size_t need = 0;
+                const size_t room = std::min(L.cap - std::min(L.cap, L.used), S->arena.largest());
                 while (!L.pending.empty() && (int)s.reqs.size() < L.max_batch) {
-                    Req *r = L.pending.front();
-                    const size_t need = 2 * ((r->bytes + 255) / 256 * 256);
-                    if (used + need > s.io_cap) break;
-                    used += need;
-                    s.reqs.push_back(r);
+                    s.reqs.push_back(L.pending.front());
+                    const size_t n = launch_bytes(s.reqs, s.cfg);
+                    if (n > room) {
+                        s.reqs.pop_back();
+                        break;
+                    }
+                    need = n;
                     L.pending.pop_front();
                 }
                 if (s.reqs.empty()) continue;
+                if (!S->arena.alloc(need, &s.blk_off)) {  // not reached: need <= the largest free block
+                    for (auto it = s.reqs.rbegin(); it != s.reqs.rend(); ++it) L.pending.push_front(*it);
+                    s.reqs.clear();
+                    continue;
+                }
+                s.blk_len = need;
+                L.used += need;
                 s.busy = true;
                 S->in_flight += s.reqs.size();
                 lk.unlock();
@@ -157,7 +244,10 @@ void dispatcher_loop(bgt_server *S)
                 lk.lock();
                 if (rc == BGT_OK) s.launched = true;
                 if (rc != BGT_OK) {
-                    // the slot's requests fail; the slot is free again
+                    // the slot's requests fail; the slot and its block are free again
+                    cudaStreamSynchronize(s.stream);
+                    S->arena.release(s.blk_off, s.blk_len);
+                    L.used -= s.blk_len;
                     const double t = now_ms();
                     for (Req *r : s.reqs) {
                         r->status = rc;
@@ -213,6 +303,8 @@ void completer_loop(bgt_server *S)
                 }
                 S->in_flight -= s.reqs.size();
                 s.reqs.clear();
+                S->arena.release(s.blk_off, s.blk_len);
+                L.used -= s.blk_len;
                 s.busy = false;
                 s.launched = false;
                 any = true;
@@ -223,35 +315,28 @@ void completer_loop(bgt_server *S)
     }
 }
 
-int setup_lane(bgt_server *S, int li, int dims, int priority, int nslots, int max_batch, size_t io_cap,
-               size_t pool_bytes, int grid_cap, int cfg)
+int setup_lane(bgt_server *S, int li, int dims, int priority, int nslots, int max_batch, size_t cap, int grid_cap,
+               int cfg)
 {
     Lane &L = S->lane[li];
     L.dims = dims;
     L.max_batch = max_batch;
-    L.pool_bytes = pool_bytes;
+    L.cap = cap;
     L.slots.resize(nslots);
     for (Slot &s : L.slots) {
         s.cfg = cfg;
-        if (S->reserved + io_cap + pool_bytes > S->budget)
-            return fail(BGT_ERR_LIMIT, "serving slots exceed the HBM budget (%zu bytes)", S->budget);
         int rc = bgt_ctx_create(S->device, &s.ctx);
         if (rc != BGT_OK) return rc;
         cudaError_t e = cudaStreamCreateWithPriority(&s.stream, cudaStreamNonBlocking, priority);
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreateWithPriority");
         bgt_ctx_set_stream(s.ctx, s.stream);
         if ((rc = bgt_batch_create(s.ctx, &s.b)) != BGT_OK) return rc;
-        if ((rc = bgt_batch_reserve(s.b, pool_bytes)) != BGT_OK) return rc;
         bgt_batch_set_grid(s.b, grid_cap);
         // tile rings: the lanes share the SMs with one another, which the
         // resident kernel (one 225 KB CTA on every SM at once) cannot
         bgt_batch_set_engine(s.b, 1);
-        e = cudaMalloc(&s.d_io, io_cap);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(serving staging)");
-        s.io_cap = io_cap;
         e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
         if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
-        S->reserved += io_cap + pool_bytes;
     }
     return BGT_OK;
 }
@@ -262,13 +347,14 @@ void teardown(bgt_server *S)
         for (Slot &s : L.slots) {
             if (s.stream) cudaStreamSynchronize(s.stream);
             if (s.b) bgt_batch_destroy(s.b);
-            if (s.d_io) cudaFree(s.d_io);
             if (s.done) cudaEventDestroy(s.done);
             if (s.ctx) bgt_ctx_destroy(s.ctx);
             if (s.stream) cudaStreamDestroy(s.stream);
         }
         L.slots.clear();
     }
+    if (S->arena.base) cudaFree(S->arena.base);
+    S->arena = Arena();
     // every request not yet returned by a poll is still in `live`
     for (auto &kv : S->live) delete kv.second;
     S->live.clear();
@@ -277,9 +363,8 @@ void teardown(bgt_server *S)
 
 }  // namespace
 
-// Lane 0 serves 2D requests, up to 16 per launch (any frame up to about
-// 16 MB of pixels); lane 1 serves 3D requests, up to 4 per launch (volumes
-// up to 320^3 uint8).  Slot memory is reserved here, within hbm_budget_bytes.
+// Lane 0 serves 2D requests, up to 16 per launch; lane 1 serves 3D requests,
+// up to 4 per launch.  The arena (hbm_budget_bytes) is allocated here.
 extern "C" int bgt_server_create(int device, size_t hbm_budget_bytes, bgt_server **out)
 {
     if (!out) return fail(BGT_ERR_ARG, "null out");
@@ -294,14 +379,22 @@ extern "C" int bgt_server_create(int device, size_t hbm_budget_bytes, bgt_server
     S->device = device;
     S->budget = hbm_budget_bytes;
     const size_t MiB = size_t(1) << 20;
-    // frames: 16 x (1024^2 in + out) per slot, packed pools are small; two
-    // slots with one CTA per SM each
-    int rc = setup_lane(S, 0, 2, hi, 2, 16, 16 * 2 * MiB + 8 * MiB, 64 * MiB, sms, -1);
-    // volumes: 4 x 320^3 in + out per slot; three slots with one CTA per SM
-    // each, so frames always find room on every SM.  Volumes use 16-plane
-    // tiles: the least total work per pass (fewest halo planes), which is
-    // what a throughput lane sharing the GPU with latency-bound frames wants
-    if (rc == BGT_OK) rc = setup_lane(S, 1, 3, lo, 3, 4, 4 * 2 * 33 * MiB, 192 * MiB, sms, 17);
+    e = cudaMalloc(&S->arena.base, hbm_budget_bytes);
+    if (e != cudaSuccess) {
+        delete S;
+        return cuda_fail(e, "cudaMalloc(serving arena)");
+    }
+    S->arena.size = hbm_budget_bytes;
+    S->arena.free[0] = hbm_budget_bytes;
+    // volumes leave room for one launch of 16 megapixel frames
+    const size_t guard = std::min(hbm_budget_bytes / 4, size_t(64) * MiB);
+    // frames: two slots with one CTA per SM each
+    int rc = setup_lane(S, 0, 2, hi, 2, 16, hbm_budget_bytes, sms, -1);
+    // volumes: three slots with one CTA per SM each, so frames always find
+    // room on every SM.  Volumes use 16-plane tiles: the least total work per
+    // pass (fewest halo planes), which is what a throughput lane sharing the
+    // GPU with latency-bound frames wants
+    if (rc == BGT_OK) rc = setup_lane(S, 1, 3, lo, 3, 4, hbm_budget_bytes - guard, sms, 17);
     if (rc != BGT_OK) {
         teardown(S);
         delete S;
@@ -332,9 +425,10 @@ extern "C" int bgt_server_submit(bgt_server *S, int dtype, const void *host_in, 
     r->bytes = es * (size_t)w * h * d;
     r->t_submit = now_ms();
     Lane &L = S->lane[r->dims == 2 ? 0 : 1];
-    if (2 * ((r->bytes + 255) / 256 * 256) > L.slots[0].io_cap) {
+    const size_t need = launch_bytes(std::vector<Req *>{r}, L.slots[0].cfg);
+    if (need > L.cap) {
         delete r;
-        return fail(BGT_ERR_LIMIT, "request of %zu bytes exceeds the serving slot capacity", es * (size_t)w * h * d);
+        return fail(BGT_ERR_LIMIT, "request needs %zu bytes of device memory; its lane may hold %zu", need, L.cap);
     }
     {
         std::lock_guard<std::mutex> lk(S->mu);
@@ -404,6 +498,18 @@ extern "C" int bgt_server_stats(bgt_server *S, int lane, double *p50_ms, double 
     if (p99_ms) *p99_ms = pct(0.99);
     if (mvox_per_s) *mvox_per_s = L.t_last > L.t_first ? L.voxels / ((L.t_last - L.t_first) * 1e-3) / 1e6 : 0.0;
     if (completed) *completed = L.done;
+    return BGT_OK;
+}
+
+// Device memory of the server: arena bytes held by launches in flight, the
+// arena's size, and requests waiting for admission (both lanes).
+extern "C" int bgt_server_memory(bgt_server *S, size_t *used, size_t *budget, unsigned long long *waiting)
+{
+    if (!S) return fail(BGT_ERR_ARG, "null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (used) *used = S->arena.used;
+    if (budget) *budget = S->arena.size;
+    if (waiting) *waiting = S->lane[0].pending.size() + S->lane[1].pending.size();
     return BGT_OK;
 }
 

@@ -5,10 +5,10 @@ Workload: 16 concurrent streams of 1024x1024 frames at 30 fps (strokes
 displaced <= 2 px per frame, radius jitter +/-0.5 px) are 70% of the
 requests; tree volumes with sides U[128,320] are the other 30%.  Arrivals
 are a Poisson process at the combined rate (480 frames/s / 0.7).  Device
-memory is reserved once within the HBM budget (64 GB by default) and stays
-resident; the runtime admits requests into free slots as earlier ones
-finish.  Latency is measured per request from submission to output in host
-memory."""
+memory is one resident arena of the HBM budget (64 GB by default); the
+runtime admits a request when a slot of its lane is free and the arena has
+room for it, and frees the memory when its output is back in host memory.
+Latency is measured per request from submission to output in host memory."""
 from __future__ import annotations
 
 import ctypes as C
@@ -64,6 +64,12 @@ class Server:
 
     def reset_stats(self) -> None:
         check(lib().bgt_server_reset_stats(self.h))
+
+    def memory(self):
+        """(arena bytes held by launches in flight, arena bytes, requests waiting for admission)"""
+        u, b, w = C.c_size_t(), C.c_size_t(), C.c_ulonglong()
+        check(lib().bgt_server_memory(self.h, C.byref(u), C.byref(b), C.byref(w)))
+        return u.value, b.value, w.value
 
     def close(self):
         if self.h:

@@ -442,7 +442,23 @@ def run_bgt(args, rank, world, local):
                 "volume_mvoxel_per_s": s["volumes"]["mvoxel_per_s"],
                 "offered_requests_per_s": s["offered_rate_per_s"], "measured_seconds": s["duration_s"],
                 "latency": "submission to output in pinned host memory",
+                "admission": "by bytes against one resident arena of the budget (staging + batch pool per launch)",
             }
+            # the same frame streams with a growing share of volume requests
+            sweep = []
+            for vshare in (0.5, 0.7):
+                v = run_workload(duration_s=args.serve_seconds / 2, device=local, frame_share=1.0 - vshare)
+                sweep.append({"volume_share": vshare, "frame_p50_ms": v["frames"]["p50_ms"],
+                              "frame_p99_ms": v["frames"]["p99_ms"], "volume_p50_ms": v["volumes"]["p50_ms"],
+                              "volume_p99_ms": v["volumes"]["p99_ms"],
+                              "frames_completed": v["frames"]["completed"],
+                              "volumes_completed": v["volumes"]["completed"],
+                              "offered_requests_per_s": v["offered_rate_per_s"]})
+            line["serving"]["volume_share_sweep"] = [
+                {"volume_share": 0.3, "frame_p50_ms": s["frames"]["p50_ms"], "frame_p99_ms": s["frames"]["p99_ms"],
+                 "volume_p50_ms": s["volumes"]["p50_ms"], "volume_p99_ms": s["volumes"]["p99_ms"],
+                 "frames_completed": s["frames"]["completed"], "volumes_completed": s["volumes"]["completed"],
+                 "offered_requests_per_s": s["offered_rate_per_s"]}] + sweep
         if not args.no_centerline:
             line["centerline"] = centerline_block()
         if not args.no_configs:

@@ -185,11 +185,15 @@ int bgt_batch_plan(bgt_batch *b, int id, int *resident, int *bands);
  * volumes: depth > 1) are submitted from any host thread with host buffers
  * (pinned memory keeps the copies asynchronous) that must stay valid until
  * the request completes.  A dispatcher thread admits waiting requests into
- * free device slots of their lane (frames: high-priority streams; volumes:
- * low-priority streams) when the slot has room, and launches them while
- * earlier launches still run (continuous batching); device memory is
- * reserved once at creation within hbm_budget_bytes and stays resident.
- * Latency = submit to output in host memory. */
+ * free slots of their lane (frames: high-priority streams; volumes:
+ * low-priority streams) and launches them while earlier launches still run
+ * (continuous batching).  Device memory is one arena of hbm_budget_bytes,
+ * allocated at creation and resident; each launch holds a block of it sized
+ * from its requests (staging + batch pool) until its outputs are back in
+ * host memory, and a request waits until the arena has room for it (volumes
+ * leave a guard for one launch of frames).  A request larger than its lane
+ * may ever hold is rejected at submit with BGT_ERR_LIMIT.  Latency = submit
+ * to output in host memory. */
 typedef struct bgt_server bgt_server;
 int bgt_server_create(int device, size_t hbm_budget_bytes, bgt_server **out);
 int bgt_server_submit(bgt_server *s, int dtype, const void *host_in, int width, int height, int depth,
@@ -201,6 +205,9 @@ int bgt_server_drain(bgt_server *s, double timeout_s);
 int bgt_server_stats(bgt_server *s, int lane, double *p50_ms, double *p99_ms, double *mvox_per_s,
                      unsigned long long *completed);
 int bgt_server_reset_stats(bgt_server *s);
+/* arena bytes held by launches in flight, the arena's size, and requests
+ * waiting for admission */
+int bgt_server_memory(bgt_server *s, size_t *used, size_t *budget, unsigned long long *waiting);
 int bgt_server_destroy(bgt_server *s);
 
 /* ---- tile configurations and the autotuner's table --------------------
