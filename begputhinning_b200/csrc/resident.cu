@@ -519,30 +519,45 @@ __device__ uint32_t res_brick3d(const Vol3D &v, int s, const uint32_t *IN, uint3
     return chg;
 }
 
+// One volume, or one z-slab of a large volume: brick layers [r0, r1) are
+// the slab's core, `halo` layers on each side (clamped to the volume) are
+// held too and recomputed.  Slabs run whole iterations (pre-test, U, N, E, D,
+// S, W) in lockstep and trade their boundary layers through global memory
+// after each: errors entering at a slab's outer edge move one plane per
+// subiteration (the pre-test's union reads one plane further, inside the
+// same bound), six planes in an iteration, so a halo of two layers (eight
+// planes) keeps the core exact.  Halo bricks and the core bricks next to
+// them are processed in every iteration.
 __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S, int *take)
 {
-    (void)it;
-    __shared__ int s_cnt;
+    __shared__ int s_cnt, s_flag;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Vol3D v;
     const int wl = (in.W + 31) >> 5;
+    const int nbz_all = (in.D + kBZ - 1) / kBZ;
+    const bool banded = it.bands > 1;
+    const int c_lo = banded ? it.r0 : 0, c_hi = banded ? it.r1 : nbz_all;
+    const int e_lo = max(0, c_lo - it.halo), e_hi = min(nbz_all, c_hi + it.halo);
     v.nbx = wl;
     v.nby = (in.H + 31) >> 5;
-    v.nbz = (in.D + kBZ - 1) / kBZ;
+    v.nbz = e_hi - e_lo;
+    const int bz0 = e_lo;
     const int nb = v.nbx * v.nby * v.nbz;
     v.tab = reinterpret_cast<uint16_t *>(smb);
     for (int i = threadIdx.x; i < nb; i += kResThreads) v.tab[i] = 0;
     __syncthreads();
     // mark the non-empty bricks: one coalesced pass over the used words of
-    // the packed volume (word i of the pass = word i % wl of row i / wl)
+    // the held planes (word i of the pass = word i % wl of row i / wl)
     const uint32_t *g0 = in.buf[0];
+    const int z_first = kBZ * e_lo, z_end = min(in.D, kBZ * e_hi);
     {
-        const int nw = in.D * in.H * wl;
+        const int nw = (z_end - z_first) * in.H * wl;
+        const size_t base = (size_t)z_first * in.H;
         for (int i = threadIdx.x; i < nw; i += kResThreads) {
             const int r = i / wl, x = i - r * wl;
-            if (__ldcg(g0 + (size_t)r * in.P + x) != 0u) {
-                const int z = r / in.H, y = r - z * in.H;
-                v.tab[((z / kBZ) * v.nby + (y >> 5)) * v.nbx + x] = 1;
+            if (__ldcg(g0 + (base + r) * in.P + x) != 0u) {
+                const int zl = r / in.H, y = r - zl * in.H;
+                v.tab[((zl / kBZ) * v.nby + (y >> 5)) * v.nbx + x] = 1;
             }
         }
     }
@@ -555,7 +570,30 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
     int total = 0;
     const int first = res_block_exscan(cnt, &total);
     v.nslots = total;
-    if (res_bytes3d(nb, total) > (size_t)kSmemBytes) {
+    const bool fits = res_bytes3d(nb, total) <= (size_t)kSmemBytes;
+    if (banded) {
+        // every slab must fit, or the tile engine takes the whole volume:
+        // the slabs agree before any of them writes anything
+        if (threadIdx.x == 0) {
+            if (!fits) atomicExch(&in.spill, 1);
+            __threadfence();
+            atomicAdd(&in.res_arrive, 1);
+            int f;
+            if (!res_wait_at_least(&in.res_arrive, it.bands, S->timeout_ns)) {
+                atomicOr(&S->status, kErrQueueTimeout);
+                f = 2;
+            } else {
+                f = ld_acquire(&in.spill) ? 1 : 0;
+            }
+            s_flag = f;
+        }
+        __syncthreads();
+        if (s_flag) {
+            if (s_flag == 2 && threadIdx.x == 0) atomicMin(&in.converged, -1);
+            __syncthreads();
+            return;
+        }
+    } else if (!fits) {
         // does not fit: the tile engine thins this volume (nothing here was written to it)
         if (threadIdx.x == 0) in.spill = 1;
         __syncthreads();
@@ -594,20 +632,38 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
     }
     if (threadIdx.x < 2) take[threadIdx.x] = 0;
     __syncthreads();
-    // gather the non-empty bricks (both state buffers)
-    for (int s = warp + 1; s <= total; s += kWarps) {
+    // brick layer (global) of a slot
+    auto layer_of = [&](int s) { return bz0 + v.coord[s] / (v.nbx * v.nby); };
+    // copy the slot's words from / to packed volume g (rows inside the volume only)
+    auto gather = [&](const uint32_t *g, int s, bool both) {
         const int li = v.coord[s];
-        const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
+        const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = bz0 + li / (v.nbx * v.nby);
         const int y = 32 * by + lane;
 #pragma unroll
         for (int q = 0; q < kBZ; q++) {
             const int z = kBZ * bz + q;
-            const uint32_t w = (y < in.H && z < in.D) ? __ldcg(g0 + ((size_t)z * in.H + y) * in.P + bx) : 0u;
+            const uint32_t w = (y < in.H && z < in.D) ? __ldcg(g + ((size_t)z * in.H + y) * in.P + bx) : 0u;
             v.X[s * kSlotWords + q * 32 + lane] = w;
-            v.Y[s * kSlotWords + q * 32 + lane] = w;
+            if (both) v.Y[s * kSlotWords + q * 32 + lane] = w;
         }
-    }
+    };
+    auto scatter = [&](uint32_t *g, int s) {
+        const int li = v.coord[s];
+        const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = bz0 + li / (v.nbx * v.nby);
+        const int y = 32 * by + lane;
+        if (y >= in.H) return;
+#pragma unroll
+        for (int q = 0; q < kBZ; q++) {
+            const int z = kBZ * bz + q;
+            if (z < in.D) g[((size_t)z * in.H + y) * in.P + bx] = v.X[s * kSlotWords + q * 32 + lane];
+        }
+    };
+    // gather the non-empty bricks (both state buffers)
+    for (int s = warp + 1; s <= total; s += kWarps) gather(g0, s, true);
     __syncthreads();
+    // layers processed in every iteration of a slab: its halo and the core layers next to it
+    const int keep_lo = it.band > 0 ? c_lo + it.halo : 0;
+    const int keep_hi = it.band + 1 < it.bands ? c_hi - it.halo : nbz_all;
 
     int iter = 0, result = 0;
     unsigned long long words = 0, bricks = 0;
@@ -638,19 +694,24 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
                 }
                 if (lane == 0) {
                     const int li = v.coord[s];
-                    const int by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
-                    words += (unsigned long long)min(32, in.H - 32 * by) * min(kBZ, in.D - kBZ * bz);
-                    bricks++;
+                    const int by = (li / v.nbx) % v.nby, bz = bz0 + li / (v.nbx * v.nby);
+                    if (bz >= c_lo && bz < c_hi) {
+                        words += (unsigned long long)min(32, in.H - 32 * by) * min(kBZ, in.D - kBZ * bz);
+                        bricks++;
+                    }
                 }
                 if (__any_sync(kFull, c != 0u) && lane == 0) v.chg[s] = 1;
             }
             __syncthreads();
         }
-        // next iteration's bricks: the 3x3x3 brick neighbourhoods of the changed ones
-        int any = 0;
+        // next iteration's bricks: the 3x3x3 brick neighbourhoods of the
+        // changed ones; `core` = a core brick changed
+        int core = 0;
         for (int s = threadIdx.x + 1; s <= total; s += kResThreads) {
+            const int bzs = layer_of(s);
+            if (banded && (bzs < keep_lo || bzs >= keep_hi)) v.nxt[s] = 1;
             if (!v.chg[s]) continue;
-            any = 1;
+            if (bzs >= c_lo && bzs < c_hi) core = 1;
             const int li = v.coord[s];
             const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
             for (int dz = -1; dz <= 1; dz++) {
@@ -668,9 +729,49 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
                 }
             }
         }
-        if (!__syncthreads_or(any)) {
-            result = 1;
-            break;
+        const bool any_core = __syncthreads_or(core);
+        if (!banded) {
+            if (!any_core) {
+                result = 1;
+                break;
+            }
+        } else {
+            // trade boundary layers with the neighbouring slabs (state in X)
+            uint32_t *gx = in.buf[(iter + 1) & 1];  // buf[0] holds the start state other slabs may still load
+            for (int s = warp + 1; s <= total; s += kWarps) {
+                const int bzs = layer_of(s);
+                const bool out_lo = it.band > 0 && bzs >= c_lo && bzs < c_lo + it.halo;
+                const bool out_hi = it.band + 1 < it.bands && bzs >= c_hi - it.halo && bzs < c_hi;
+                if (out_lo || out_hi) scatter(gx, s);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                if (any_core) atomicMax(&in.res_last, iter);
+                atomicAdd(&in.res_arrive, 1);
+                int f;
+                if (!res_wait_at_least(&in.res_arrive, it.bands * (iter + 2), S->timeout_ns)) {
+                    atomicOr(&S->status, kErrQueueTimeout);
+                    f = 2;
+                } else {
+                    f = ld_acquire(&in.res_last) < iter ? 1 : 0;
+                }
+                s_flag = f;
+            }
+            __syncthreads();
+            const int f = s_flag;
+            if (f == 1) {
+                result = 1;
+                break;
+            }
+            if (f == 2) {
+                result = -1;
+                break;
+            }
+            for (int s = warp + 1; s <= total; s += kWarps) {
+                const int bzs = layer_of(s);
+                if (bzs < c_lo || bzs >= c_hi) gather(gx, s, true);
+            }
         }
         for (int s = threadIdx.x + 1; s <= total; s += kResThreads) {
             v.act[s] = v.nxt[s];
@@ -684,26 +785,19 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
         }
     }
     __syncthreads();
-    // the converged state (in X after the sixth subiteration) -> buf[0]
+    // the converged core (in X after the sixth subiteration) -> buf[0]
     uint32_t *g0w = in.buf[0];
     for (int s = warp + 1; s <= total; s += kWarps) {
-        const int li = v.coord[s];
-        const int bx = li % v.nbx, by = (li / v.nbx) % v.nby, bz = li / (v.nbx * v.nby);
-        const int y = 32 * by + lane;
-        if (y >= in.H) continue;
-#pragma unroll
-        for (int q = 0; q < kBZ; q++) {
-            const int z = kBZ * bz + q;
-            if (z < in.D) g0w[((size_t)z * in.H + y) * in.P + bx] = v.X[s * kSlotWords + q * 32 + lane];
-        }
+        const int bzs = layer_of(s);
+        if (bzs >= c_lo && bzs < c_hi) scatter(g0w, s);
     }
     if (lane == 0 && words) {
         atomicAdd(&in.work_words, words);
         atomicAdd(&in.tiles_run, bricks);
     }
     if (threadIdx.x == 0) {
-        in.passes_run = 6 * (iter + 1);
-        in.converged = result;
+        if (it.band == 0) in.passes_run = 6 * (iter + 1);
+        if (result < 0) atomicMin(&in.converged, -1);
     }
     __syncthreads();
 }

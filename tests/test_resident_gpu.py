@@ -134,3 +134,21 @@ def test_resident_small_grids(ctx, grid):
         assert p[1] <= grid
     for k, (g, it) in enumerate(zip(got, items)):
         assert np.array_equal(g, _want(it)), f"instance {k} (plan {plans[k]})"
+
+
+@pytest.mark.parametrize("slab_voxels", ["60000", "300000"])
+def test_resident_volume_slabs(ctx, slab_voxels, monkeypatch):
+    """Volumes cut into z-slabs of brick layers on separate CTAs, trading two
+    halo layers after every iteration (the slab size is lowered so that
+    small volumes are cut too)."""
+    from begputhinning_b200 import synth
+    monkeypatch.setenv("BGT_RES3D_SLAB_VOXELS", slab_voxels)
+    rng = np.random.default_rng(int(slab_voxels) % 97)
+    items = [blobs3d(rng, 96, 70, 80, 30, rmax=9), synth.trees3d(6, 96, 80, 72, ntrees=3, nell=1),
+             random3d(rng, 40, 30, 33, 0.5), blobs3d(rng, 17, 40, 40, 4)]
+    runs, plans, stats = _run(ctx, items, runs=2)
+    assert plans[0][1] > 1 and plans[1][1] > 1, plans
+    for r, got in enumerate(runs):
+        for k, (g, it) in enumerate(zip(got, items)):
+            assert np.array_equal(g, _want(it)), f"run {r} volume {k} shape {it.shape} plan {plans[k]}"
+    assert all(s["converged"] == 1 for s in stats)
