@@ -19,7 +19,7 @@ EXPORTS = [
     "bgt_batch_create", "bgt_batch_destroy", "bgt_batch_add2d", "bgt_batch_add3d", "bgt_batch_finalize",
     "bgt_batch_reserve", "bgt_batch_reset", "bgt_batch_set_grid",
     "bgt_batch_set_io", "bgt_batch_run", "bgt_batch_instance_stats", "bgt_batch_device_bytes", "bgt_batch_work", "bgt_batch_stage_ms",
-    "bgt_batch_engine_ms", "bgt_batch_set_engine", "bgt_batch_plan",
+    "bgt_batch_engine_ms", "bgt_batch_set_engine", "bgt_batch_plan", "bgt_batch_res_trace",
     "bgt_tune_class", "bgt_tune_set", "bgt_tune_get", "bgt_cfg_list", "bgt_cfg_describe", "bgt_rule_table",
     "bgt_server_create", "bgt_server_submit", "bgt_server_poll", "bgt_server_drain", "bgt_server_stats",
     "bgt_server_reset_stats", "bgt_server_destroy", "bgt_server_memory",
@@ -81,6 +81,7 @@ def _declare(L):
         "bgt_batch_engine_ms": [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)],
         "bgt_batch_set_engine": [vp, I],
         "bgt_batch_plan": [vp, I, ip, ip],
+        "bgt_batch_res_trace": [vp, ip, ip, ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), ip, I],
         "bgt_tune_class": [I, I, I, I],
         "bgt_tune_set": [I, I, I],
         "bgt_tune_get": [I, I, ip],

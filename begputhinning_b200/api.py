@@ -326,6 +326,19 @@ class Batch:
         check(lib().bgt_batch_stage_ms(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
 
+    def res_trace(self):
+        """Per work item of the resident kernel's last run, in the order taken:
+        (instance, band, start ns, end ns, SM)."""
+        n = C.c_int()
+        check(lib().bgt_batch_res_trace(self.h, C.byref(n), None, None, None, None, None, 0))
+        m = n.value
+        if m == 0:
+            return []
+        inst, band, sm = (C.c_int * m)(), (C.c_int * m)(), (C.c_int * m)()
+        t0, t1 = (C.c_longlong * m)(), (C.c_longlong * m)()
+        check(lib().bgt_batch_res_trace(self.h, C.byref(n), inst, band, t0, t1, sm, m))
+        return list(zip(inst, band, t0, t1, sm))
+
     def engine_ms(self):
         """(resident kernel, tile rings) device milliseconds of the last engine run."""
         a, b = C.c_float(), C.c_float()

@@ -357,7 +357,7 @@ struct InstOffs {
 struct PoolLayout {
     std::vector<InstOffs> offs;
     size_t off_lc = 0, lc_bytes = 0, off_io = 0, off_sched = 0, off_seq = 0, off_item = 0, off_inst = 0,
-           off_tmap = 0, off_flag = 0, off_res = 0, off_rs = 0, total = 0;
+           off_tmap = 0, off_flag = 0, off_res = 0, off_rs = 0, off_rt = 0, total = 0;
     unsigned cap = 0;
 };
 
@@ -399,6 +399,7 @@ static PoolLayout layout_pool(const std::vector<Inst> &h, size_t n_res_items)
     // resident engine: item list + its scheduler
     L.off_res = off; off = align_up(off + std::max<size_t>(1, n_res_items) * sizeof(ResItem), 256);
     L.off_rs = off; off = align_up(off + sizeof(ResSched), 256);
+    L.off_rt = off; off = align_up(off + std::max<size_t>(1, n_res_items) * sizeof(ResTrace), 256);
     L.total = off;
     return L;
 }
@@ -462,6 +463,7 @@ extern "C" int bgt_batch_finalize(bgt_batch *b)
     b->d_io = (IODesc *)(P + off_io);
     b->d_res_items = (ResItem *)(P + off_res);
     b->d_rs = (ResSched *)(P + off_rs);
+    b->d_rtrace = (ResTrace *)(P + L.off_rt);
     b->cap = cap;
     std::vector<CUtensorMap> &maps = b->maps;
     maps.assign((size_t)N * kMapsPerInst, CUtensorMap());
@@ -604,6 +606,33 @@ extern "C" int bgt_batch_engine_ms(bgt_batch *b, float *resident_ms, float *ring
     if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
     if (resident_ms) *resident_ms = r;
     if (rings_ms) *rings_ms = g;
+    return BGT_OK;
+}
+
+// Timeline of the resident kernel's work items in the last run, in the
+// order they were taken: instance, band, start and end (global timer, ns,
+// relative to the earliest start) and SM.  *n = the number of items.
+extern "C" int bgt_batch_res_trace(bgt_batch *b, int *n, int *inst, int *band, long long *t0_ns, long long *t1_ns,
+                                   int *sm, int cap)
+{
+    if (!b || !b->finalized || !n) return fail(BGT_ERR_STATE, "batch not finalized");
+    const int m = (int)b->res_items.size();
+    *n = m;
+    if (m == 0 || cap <= 0) return BGT_OK;
+    int rc = batch_check(b);
+    if (rc != BGT_OK) return rc;
+    std::vector<ResTrace> tr(m);
+    cudaError_t e = cudaMemcpy(tr.data(), b->d_rtrace, m * sizeof(ResTrace), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "trace readback");
+    long long base = tr[0].t0;
+    for (const ResTrace &t : tr) base = std::min(base, t.t0);
+    for (int k = 0; k < m && k < cap; k++) {
+        if (inst) inst[k] = b->res_items[k].inst;
+        if (band) band[k] = b->res_items[k].band;
+        if (t0_ns) t0_ns[k] = tr[k].t0 - base;
+        if (t1_ns) t1_ns[k] = tr[k].t1 - base;
+        if (sm) sm[k] = tr[k].sm;
+    }
     return BGT_OK;
 }
 
@@ -771,7 +800,7 @@ static int enqueue_engine(bgt_batch *b, cudaStream_t st, bool capturing)
     // bands of an image wait for one another only for the length of one
     // iteration of the slowest band: 4 s is far beyond any legitimate wait
     e = launch_resident(b->res_grid, b->d_insts, N, b->d_res_items, (int)b->res_items.size(), b->d_rs,
-                        4000000000LL, st);
+                        b->d_rtrace, 4000000000LL, st);
     if (e != cudaSuccess) return cuda_fail(e, "resident engine launch");
     stage_event(b->ev[2], st, capturing);
     if (b->any_ring || b->any_res3d) {

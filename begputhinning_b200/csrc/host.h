@@ -126,6 +126,7 @@ struct bgt_batch {
     std::vector<bgt::ResItem> res_items;
     bgt::ResItem *d_res_items = nullptr;
     bgt::ResSched *d_rs = nullptr;
+    bgt::ResTrace *d_rtrace = nullptr;  // per-item timeline of the last resident run
     int res_grid = 0;
     bool any_ring = false;            // some instance is planned for the tile rings
     bool any_res3d = false;           // some volume may spill from the resident engine to the rings

@@ -63,6 +63,11 @@ struct ResSched {
     int pad;
     long long timeout_ns;
 };
+// Timeline of one work item of the last run (global timer, ns; SM id).
+struct ResTrace {
+    long long t0, t1;
+    int sm, pad;
+};
 constexpr int kResThreads = 512;
 // Dynamic shared memory of the resident kernel (one CTA per SM).
 int res_smem_bytes();
@@ -72,7 +77,7 @@ int res_rows_fit2d(int W);
 bool res_fits3d(int W, int H, int D);
 cudaError_t res_occupancy(int *per_sm);  // resident CTAs per SM
 cudaError_t launch_resident(int grid, Inst *d_insts, int ninst, const ResItem *d_items, int nitems,
-                            ResSched *d_rs, long long timeout_ns, cudaStream_t st);
+                            ResSched *d_rs, ResTrace *d_trace, long long timeout_ns, cudaStream_t st);
 
 // Per-instance input/output of a batch-wide pack/unpack launch.
 // Unsigned 32-bit division by a divisor fixed per instance, as a multiply

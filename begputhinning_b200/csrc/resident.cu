@@ -825,7 +825,15 @@ __global__ void resident_reset_kernel(Inst *insts, int n, ResSched *S, int nitem
     }
 }
 
-__global__ void __launch_bounds__(kResThreads, 1) resident_kernel(Inst *insts, const ResItem *items, ResSched *S)
+__device__ __forceinline__ int res_smid()
+{
+    int v;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(v));
+    return v;
+}
+
+__global__ void __launch_bounds__(kResThreads, 1)
+    resident_kernel(Inst *insts, const ResItem *items, ResSched *S, ResTrace *trace)
 {
     extern __shared__ __align__(16) uint8_t res_smem[];
     __shared__ int s_item;
@@ -838,10 +846,12 @@ __global__ void __launch_bounds__(kResThreads, 1) resident_kernel(Inst *insts, c
         if (k >= S->nitems) break;
         const ResItem it = items[k];
         Inst &in = insts[it.inst];
+        const long long t0 = (long long)globaltimer();
         if (in.dims == 2)
             res_run2d(in, it, reinterpret_cast<uint32_t *>(res_smem), S, s_take);
         else
             res_run3d(in, it, res_smem, S, s_take);
+        if (threadIdx.x == 0) trace[k] = ResTrace{t0, (long long)globaltimer(), res_smid(), 0};
     }
 }
 
@@ -853,7 +863,7 @@ cudaError_t res_occupancy(int *per_sm)
 }
 
 cudaError_t launch_resident(int grid, Inst *d_insts, int ninst, const ResItem *d_items, int nitems,
-                            ResSched *d_rs, long long timeout_ns, cudaStream_t st)
+                            ResSched *d_rs, ResTrace *d_trace, long long timeout_ns, cudaStream_t st)
 {
     static bool attr_done = false;
     if (!attr_done) {
@@ -877,7 +887,7 @@ cudaError_t launch_resident(int grid, Inst *d_insts, int ninst, const ResItem *d
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, resident_kernel, d_insts, d_items, d_rs);
+    return cudaLaunchKernelEx(&cfg, resident_kernel, d_insts, d_items, d_rs, d_trace);
 }
 
 }  // namespace bgt

@@ -179,6 +179,13 @@ int bgt_batch_set_engine(bgt_batch *b, int mode);
 /* Plan of instance id after finalize: *resident = 1 when the resident
  * kernel takes it, *bands = the CTAs a 2D image is cut into (0 for rings). */
 int bgt_batch_plan(bgt_batch *b, int id, int *resident, int *bands);
+/* Timeline of the resident kernel's work items in the last run (no
+ * reference counterpart; for tracing load balance): per item, in the order
+ * taken, its instance, band, start and end in ns from the earliest start
+ * (device global timer) and the SM that ran it.  *n = number of items; at
+ * most cap are written.  Synchronises the batch's stream. */
+int bgt_batch_res_trace(bgt_batch *b, int *n, int *inst, int *band, long long *t0_ns, long long *t1_ns, int *sm,
+                        int cap);
 
 /* ---- serving -------------------------------------------------------------
  * A request loop over the batch engine.  Requests (2D frames: depth 1; 3D
