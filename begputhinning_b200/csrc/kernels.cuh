@@ -68,7 +68,7 @@ struct ResTrace {
     long long t0, t1;
     int sm, pad;
 };
-constexpr int kResThreads = 512;
+constexpr int kResThreads = 768;
 // Dynamic shared memory of the resident kernel (one CTA per SM).
 int res_smem_bytes();
 // Rows of a W-wide 2D band (core plus halo) that one CTA holds.

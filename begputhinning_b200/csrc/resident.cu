@@ -1,24 +1,23 @@
 // resident.cu -- the resident engine: every work item (an instance, or one
 // band of rows of a 2D image too large for one CTA) is loaded once into one
 // CTA's shared memory and thinned there from its first subiteration to its
-// fixed point; only the bands of a large image meet, once per iteration, to
-// trade boundary rows through global memory.  One CTA of 512 threads per SM
-// holds up to 225 KB.
+// fixed point; only the bands of a large image (or slabs of a large volume)
+// meet, once per iteration, to trade boundary rows through global memory.
+// One CTA of 768 threads per SM holds up to 225 KB.
 //
 // 2D band (dense).  Rows of the band (core plus `halo` rows on each side,
-// clamped to the image) lie in shared memory with an odd pitch of
-// 2*ceil(wl/2)+3 words (wl = ceil(W/32); a zero word left of every row and
-// zero words right of it).  A subiteration processes strips of 32 rows, one
-// warp per strip, lane = row, walking the row in pairs of words: each lane
+// clamped to the image) lie twice in shared memory (subiteration t reads one
+// copy and writes the other) with an odd pitch of 2*ceil(wl/2)+3 words
+// (wl = ceil(W/32); a zero word left of every row and zero words right of
+// it).  A subiteration hands units (a strip of 32 rows x a chunk of words,
+// chunks sized so that there are about two units per warp) to warps
+// dynamically; lane = row, walking the chunk in pairs of words: each lane
 // loads its own row and the rows above and below straight from shared
-// memory and forms the x-neighbours by funnel shifts.  Rows are updated in
-// place: within a warp the loads of a step precede its stores (__syncwarp),
-// and the rows just outside a strip (read by its lanes 0 and 31) come from a
-// copy of every strip's first and last rows taken at the end of the previous
-// subiteration (double-buffered by parity), so no warp reads a row another
-// warp is rewriting.  A strip whose neighbourhood (itself and the strips above
-// and below) did not change during the last four subiterations -- one of
-// each direction -- is a fixed point for the next one and is skipped.  A
+// memory and forms the x-neighbours by funnel shifts.  A unit whose 3x3
+// neighbourhood of units did not change during the last four subiterations
+// -- one of each direction -- is a fixed point for the next one and is
+// skipped (a unit processed without a change wrote identical data to both
+// copies, so a skipped unit is current in both).  A
 // single band stops after four consecutive subiterations without a deletion
 // (a fixed point of N, S, E and W: the reference's result, whatever the
 // alignment).  Bands of one image run their iterations (N, S, E, W) in
@@ -69,13 +68,15 @@ __host__ __device__ inline int res_pitch2d(int W)
     return 2 * ((wl + 1) >> 1) + 3;
 }
 
-// words of shared memory a band of nrows rows needs: zero row, rows, edge
-// copies (2 parities x 2 rows per strip) and the per-strip change record
+// words of shared memory a band of nrows rows needs: zero row, two row
+// buffers and the change record of its units (at most one per 4 words of a
+// strip)
 __host__ __device__ inline size_t res_words2d(int W, int nrows)
 {
     const int pp = res_pitch2d(W);
     const int ns = (nrows + 31) >> 5;
-    return (size_t)pp * (1 + (size_t)nrows + 4 * (size_t)ns) + (size_t)ns;
+    const int wl = (W + 31) >> 5;
+    return (size_t)pp * (1 + 2 * (size_t)nrows) + (size_t)ns * ((wl + 3) / 4);
 }
 
 // bytes of shared memory a volume with nb bricks of which ns are non-empty needs
@@ -151,29 +152,31 @@ __device__ int res_block_exscan(int v, int *total)
 // ------------------------------------------------------------ 2D ----------
 struct Band2D {
     uint32_t *zero;     // pp zero words
-    uint32_t *rows;     // nrows x pp
-    uint32_t *E;        // [2 parities][nstrips][first, last row][pp]
-    int *lastchg;       // per strip: last subiteration with a deletion
+    uint32_t *buf[2];   // nrows x pp each: subiteration t reads buf[t & 1], writes buf[(t + 1) & 1]
+    int *lastchg;       // [nstrips][nchunks]: last subiteration with a deletion in the unit
     int pp, npairs, wl, nrows, nstrips;
+    int cw, nchunks;    // words per chunk (even) and chunks per row
     int a;              // image row of the band's first row in shared memory
     int r0, r1;         // core rows (image coordinates)
 };
 
-// One subiteration of direction DIR on one strip's row (this lane's), in
-// place.  own/up/dn: this row and the rows above and below (pass-start
-// values; the row pointers of lanes 0 and 31 point at edge copies).  Words
-// 0 and 2*npairs+1.. are zero pads.  Returns the deleted bits.
+// Subiteration of direction DIR on words [w0, w0 + 2*np) of this lane's row
+// (w0 odd), from the pass-start rows in/up/dn to `out` (another buffer).
+// Returns the deleted bits.
 template <int DIR>
-__device__ __forceinline__ uint32_t res_row2d(uint32_t *own, const uint32_t *up, const uint32_t *dn, bool store,
-                                              int npairs)
+__device__ __forceinline__ uint32_t res_row2d(const uint32_t *__restrict__ in, const uint32_t *__restrict__ up,
+                                              const uint32_t *__restrict__ dn, uint32_t *__restrict__ out,
+                                              bool store, int w0, int np)
 {
-    uint32_t ao = own[0], bo = own[1], au = up[0], bu = up[1], ad = dn[0], bd = dn[1];
+    uint32_t ao = in[w0 - 1], bo = in[w0], au = up[w0 - 1], bu = up[w0], ad = dn[w0 - 1], bd = dn[w0];
     uint32_t chg = 0;
-    for (int k = 0; k < npairs; k++) {
-        const int j = 2 * k + 1;
-        const uint32_t co = own[j + 1], eo = own[j + 2];
+#pragma unroll 2
+    for (int k = 0; k < np; k++) {
+        const int j = w0 + 2 * k;
+        const uint32_t co = in[j + 1], eo = in[j + 2];
         const uint32_t cu = up[j + 1], eu = up[j + 2];
         const uint32_t cd = dn[j + 1], ed = dn[j + 2];
+        uint32_t n0 = bo, n1 = co;
         if (__any_sync(kFull, (bo | co) != 0u)) {
             uint32_t X[8];
             X[0] = bu;
@@ -184,7 +187,7 @@ __device__ __forceinline__ uint32_t res_row2d(uint32_t *own, const uint32_t *up,
             X[5] = at_xm1(bd, ad);
             X[6] = at_xm1(bo, ao);
             X[7] = at_xm1(bu, au);
-            const uint32_t n0 = bo & ~rule2d<DIR>(X);
+            n0 = bo & ~rule2d<DIR>(X);
             uint32_t Y[8];
             Y[0] = cu;
             Y[1] = at_xp1(cu, eu);
@@ -194,13 +197,12 @@ __device__ __forceinline__ uint32_t res_row2d(uint32_t *own, const uint32_t *up,
             Y[5] = at_xm1(cd, bd);
             Y[6] = at_xm1(co, bo);
             Y[7] = at_xm1(cu, bu);
-            const uint32_t n1 = co & ~rule2d<DIR>(Y);
-            __syncwarp();  // every lane has read words j .. j+2 of its neighbours' rows
-            if (store) {
-                own[j] = n0;
-                own[j + 1] = n1;
-            }
+            n1 = co & ~rule2d<DIR>(Y);
             chg |= (n0 ^ bo) | (n1 ^ co);
+        }
+        if (store) {
+            out[j] = n0;
+            out[j + 1] = n1;
         }
         ao = co;
         bo = eo;
@@ -212,49 +214,42 @@ __device__ __forceinline__ uint32_t res_row2d(uint32_t *own, const uint32_t *up,
     return chg;
 }
 
-__device__ __forceinline__ void res_copy_edges2d(const Band2D &b, uint32_t *En, int s)
-{
-    const int lane = threadIdx.x & 31;
-    const uint32_t *top = b.rows + (size_t)(32 * s) * b.pp;
-    const uint32_t *bot = b.rows + (size_t)min(32 * s + 31, b.nrows - 1) * b.pp;
-    uint32_t *et = En + (size_t)(2 * s) * b.pp, *eb = et + b.pp;
-    for (int w = lane; w < b.pp; w += 32) {
-        et[w] = top[w];
-        eb[w] = bot[w];
-    }
-}
-
-// One subiteration t (direction DIR = t % 4) over the band's strips.
-// Returns this thread's deleted core bits; adds processed words to *words.
+// One subiteration t (direction DIR = t % 4) over the band's units (strip of
+// 32 rows x chunk of cw words).  A unit whose 3x3 neighbourhood of units had
+// no deletion during the last four subiterations is skipped: its
+// neighbourhood is a fixed point of the next direction, and a unit processed
+// without a change wrote identical data to both buffers.  Returns this
+// thread's deleted core bits; adds processed words to *words.
 template <int DIR>
 __device__ uint32_t res_subit2d(const Band2D &b, int t, int *take, unsigned long long *words)
 {
     const int lane = threadIdx.x & 31;
-    const size_t par = (size_t)2 * b.nstrips * b.pp;
-    const uint32_t *Ec = b.E + (t & 1) * par;
-    uint32_t *En = b.E + ((t + 1) & 1) * par;
+    const uint32_t *IN = b.buf[t & 1];
+    uint32_t *OUT = b.buf[(t + 1) & 1];
+    const int nunits = b.nstrips * b.nchunks;
     uint32_t core = 0;
     for (;;) {
-        const int s = res_take(take);
-        if (s >= b.nstrips) break;
-        const int lc = max(b.lastchg[s], max(s > 0 ? b.lastchg[s - 1] : kLongAgo,
-                                             s + 1 < b.nstrips ? b.lastchg[s + 1] : kLongAgo));
-        if (lc >= t - 4) {
-            const int r = 32 * s + lane;
-            const bool valid = r < b.nrows;
-            uint32_t *own = valid ? b.rows + (size_t)r * b.pp : b.zero;
-            const uint32_t *up = lane == 0 ? (s > 0 ? Ec + (size_t)(2 * s - 1) * b.pp : b.zero)
-                                           : (r - 1 < b.nrows ? b.rows + (size_t)(r - 1) * b.pp : b.zero);
-            const uint32_t *dn = lane == 31 ? (s + 1 < b.nstrips ? Ec + (size_t)(2 * s + 2) * b.pp : b.zero)
-                                            : (r + 1 < b.nrows ? b.rows + (size_t)(r + 1) * b.pp : b.zero);
-            const uint32_t chg = res_row2d<DIR>(own, up, dn, valid, b.npairs);
-            if (__any_sync(kFull, chg != 0u) && lane == 0) b.lastchg[s] = t;
-            const int gy = b.a + r;
-            if (valid && gy >= b.r0 && gy < b.r1) core |= chg;
-            if (lane == 0) *words += (unsigned long long)min(32, b.nrows - 32 * s) * b.wl;
-        }
-        __syncwarp();
-        res_copy_edges2d(b, En, s);
+        const int u = res_take(take);
+        if (u >= nunits) break;
+        const int s = u / b.nchunks, c = u - s * b.nchunks;
+        int lc = kLongAgo;
+        for (int ds = max(0, s - 1); ds <= min(b.nstrips - 1, s + 1); ds++)
+            for (int dc = max(0, c - 1); dc <= min(b.nchunks - 1, c + 1); dc++)
+                lc = max(lc, b.lastchg[ds * b.nchunks + dc]);
+        if (lc < t - 4) continue;
+        const int r = 32 * s + lane;
+        const bool valid = r < b.nrows;
+        const uint32_t *in = valid ? IN + (size_t)r * b.pp : b.zero;
+        const uint32_t *up = (r >= 1 && r - 1 < b.nrows) ? IN + (size_t)(r - 1) * b.pp : b.zero;
+        const uint32_t *dn = r + 1 < b.nrows ? IN + (size_t)(r + 1) * b.pp : b.zero;
+        uint32_t *out = OUT + (size_t)min(r, b.nrows - 1) * b.pp;
+        const int w0 = 1 + c * b.cw;
+        const int np = (min(b.cw, b.wl - c * b.cw) + 1) >> 1;
+        const uint32_t chg = res_row2d<DIR>(in, up, dn, out, valid, w0, np);
+        if (__any_sync(kFull, chg != 0u) && lane == 0) b.lastchg[u] = t;
+        const int gy = b.a + r;
+        if (valid && gy >= b.r0 && gy < b.r1) core |= chg;
+        if (lane == 0) *words += (unsigned long long)min(32, b.nrows - 32 * s) * min(b.cw, b.wl - c * b.cw);
     }
     return core;
 }
@@ -273,31 +268,38 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
     const int bend = min(in.H, it.r1 + it.halo);
     b.nrows = bend - b.a;
     b.nstrips = (b.nrows + 31) >> 5;
+    // chunks: enough units per subiteration for the CTA's warps (about two
+    // each), at least 4 words (2 pairs) per chunk
+    {
+        const int want = (2 * kWarps + b.nstrips - 1) / b.nstrips;
+        int cw = (b.wl + want - 1) / want;
+        cw = max(4, (cw + 1) & ~1);
+        b.cw = cw;
+        b.nchunks = (b.wl + cw - 1) / cw;
+    }
     b.zero = sm;
-    b.rows = sm + b.pp;
-    b.E = b.rows + (size_t)b.nrows * b.pp;
-    b.lastchg = reinterpret_cast<int *>(b.E + (size_t)4 * b.nstrips * b.pp);
+    b.buf[0] = sm + b.pp;
+    b.buf[1] = b.buf[0] + (size_t)b.nrows * b.pp;
+    b.lastchg = reinterpret_cast<int *>(b.buf[1] + (size_t)b.nrows * b.pp);
     const int pp = b.pp;
+    const int nunits = b.nstrips * b.nchunks;
 
     for (int i = threadIdx.x; i < pp; i += kResThreads) b.zero[i] = 0u;
-    for (int i = threadIdx.x; i < b.nstrips; i += kResThreads) b.lastchg[i] = kLongAgo;
+    for (int i = threadIdx.x; i < nunits; i += kResThreads) b.lastchg[i] = kLongAgo;
     if (threadIdx.x < 2) take[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t *g0 = in.buf[0];
     for (int r = warp; r < b.nrows; r += kWarps) {
         const uint32_t *grow = g0 + (size_t)(b.a + r) * in.P;
-        uint32_t *srow = b.rows + (size_t)r * pp;
-        uint32_t any = 0;
+        uint32_t *r0p = b.buf[0] + (size_t)r * pp, *r1p = b.buf[1] + (size_t)r * pp;
         for (int w = lane; w < pp; w += 32) {
             const uint32_t v = (w >= 1 && w <= b.wl) ? __ldcg(grow + (w - 1)) : 0u;
-            srow[w] = v;
-            any |= v;
+            r0p[w] = v;
+            r1p[w] = v;
+            // units holding foreground start as "changed just before t = 0"
+            if (v && w <= b.wl) b.lastchg[(r >> 5) * b.nchunks + (w - 1) / b.cw] = -1;
         }
-        // strips holding foreground start as "changed just before t = 0"
-        if (__any_sync(kFull, any != 0u) && lane == 0) b.lastchg[r >> 5] = -1;
     }
-    __syncthreads();
-    for (int s = warp; s < b.nstrips; s += kWarps) res_copy_edges2d(b, b.E, s);
     __syncthreads();
 
     int last_any = -1;  // last subiteration with a core deletion (same in every thread)
@@ -323,15 +325,17 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
                 break;
             }
         } else if ((t & 3) == 3) {
-            // end of iteration p: trade boundary rows with the neighbouring bands
+            // end of iteration p (state in buf[(t+1)&1]): trade boundary rows
+            // with the neighbouring bands
             const int p = t >> 2;
             const int h = it.halo;
+            uint32_t *cur = b.buf[(t + 1) & 1];
             uint32_t *gx = in.buf[(p + 1) & 1];  // buf[0] holds the start state other bands may still load
             for (int k = warp; k < 2 * h; k += kWarps) {
                 const bool top = k < h;
                 if (top ? it.band == 0 : it.band + 1 == it.bands) continue;
                 const int gy = top ? b.r0 + k : b.r1 - 2 * h + k;
-                const uint32_t *srow = b.rows + (size_t)(gy - b.a) * pp;
+                const uint32_t *srow = cur + (size_t)(gy - b.a) * pp;
                 uint32_t *grow = gx + (size_t)gy * in.P;
                 for (int w = lane; w < b.wl; w += 32) grow[w] = srow[w + 1];
             }
@@ -365,7 +369,7 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
             for (int k = warp; k < nh; k += kWarps) {
                 const int r = k < ntop ? k : (b.r1 - b.a) + (k - ntop);
                 const uint32_t *grow = gx + (size_t)(b.a + r) * in.P;
-                uint32_t *srow = b.rows + (size_t)r * pp;
+                uint32_t *srow = cur + (size_t)r * pp;
                 for (int w = lane; w < b.wl; w += 32) {
                     const uint32_t v = __ldcg(grow + w);
                     hc |= v ^ srow[w + 1];
@@ -373,14 +377,11 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
                 }
             }
             if (__syncthreads_or(hc != 0u)) {
-                // the strips holding halo rows changed: mark them and refresh
-                // their edge copies for subiteration t + 1
-                uint32_t *En = b.E + ((t + 1) & 1) * (size_t)2 * b.nstrips * pp;
-                for (int s = warp; s < b.nstrips; s += kWarps) {
-                    const int ga = b.a + 32 * s, gb = b.a + min(32 * s + 32, b.nrows);
-                    if (ga >= b.r0 && gb <= b.r1) continue;
-                    if (lane == 0) b.lastchg[s] = t;
-                    res_copy_edges2d(b, En, s);
+                // the units holding halo rows changed
+                for (int u = threadIdx.x; u < nunits; u += kResThreads) {
+                    const int st = u / b.nchunks;
+                    const int ga = b.a + 32 * st, gb = b.a + min(32 * st + 32, b.nrows);
+                    if (ga < b.r0 || gb > b.r1) b.lastchg[u] = t;
                 }
                 __syncthreads();
             }
@@ -391,11 +392,12 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
             break;
         }
     }
-    // the converged core rows -> buf[0]
+    // the converged core rows (in buf[(t+1)&1]) -> buf[0]
     __syncthreads();
+    const uint32_t *fin = b.buf[(t + 1) & 1];
     uint32_t *g0w = in.buf[0];
     for (int r = b.r0 - b.a + warp; r < b.r1 - b.a; r += kWarps) {
-        const uint32_t *srow = b.rows + (size_t)r * pp;
+        const uint32_t *srow = fin + (size_t)r * pp;
         uint32_t *grow = g0w + (size_t)(b.a + r) * in.P;
         for (int w = lane; w < b.wl; w += 32) grow[w] = srow[w + 1];
     }
