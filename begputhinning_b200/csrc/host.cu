@@ -277,16 +277,26 @@ static void plan_resident(bgt_batch *b)
     std::stable_sort(imgs.begin(), imgs.end(), [](auto &x, auto &y) { return x.first > y.first; });
     // a large volume is cut into z-slabs of whole brick layers (4 planes),
     // each with two halo layers on either side, so its iterations spread
-    // over several SMs; at least 4 core layers per slab
+    // over several SMs, and so that a slab's non-empty bricks fit one CTA
+    // (counted on the device: a volume is planned for a quarter of its
+    // slab's bricks being non-empty; one that exceeds it goes to the tile
+    // rings); at least 4 core layers per slab
     constexpr int kHalo3 = 2, kMinLayers = 4;
     double vox_per_slab = 1.0e6;
     if (const char *e = getenv("BGT_RES3D_SLAB_VOXELS")) vox_per_slab = std::max(1.0e4, atof(e));
     for (auto &v : vols) {
         const BatchItem &it = b->items[v.second];
         const int layers = (it.D + 3) / 4;
-        int G = (int)std::ceil(v.first / vox_per_slab);
-        G = std::max(1, std::min({G, layers / kMinLayers, b->res_grid}));
-        while (G > 1 && !res_fits3d(it.W, it.H, 4 * ((layers + G - 1) / G + 2 * kHalo3))) G--;
+        const int gmax = std::max(1, std::min(layers / kMinLayers, b->res_grid));
+        int G = std::max(1, std::min((int)std::ceil(v.first / vox_per_slab), gmax));
+        auto slab_ok = [&](int g) {
+            const int sl = g == 1 ? layers : (layers + g - 1) / g + 2 * kHalo3;
+            const int cap = res_slots_fit3d(it.W, it.H, 4 * sl);
+            const double bricks = (double)((it.W + 31) / 32) * ((it.H + 31) / 32) * sl;
+            return cap > 0 && 0.25 * bricks <= cap;
+        };
+        while (G < gmax && !slab_ok(G)) G++;
+        while (G > 1 && res_slots_fit3d(it.W, it.H, 4 * ((layers + G - 1) / G + 2 * kHalo3)) == 0) G--;
         for (int k = 0; k < G; k++) {
             const int r0 = (int)((long long)k * layers / G), r1 = (int)((long long)(k + 1) * layers / G);
             b->res_items.push_back(ResItem{v.second, k, G, r0, r1, G > 1 ? kHalo3 : 0});

@@ -68,11 +68,15 @@ struct ResTrace {
     long long t0, t1;
     int sm, pad;
 };
-constexpr int kResThreads = 768;
+constexpr int kResThreads = 384;
+constexpr int kResCtasPerSm = 2;
+constexpr int kResSmemBytes = 113664;  // dynamic shared memory of one CTA (two per SM)
 // Dynamic shared memory of the resident kernel (one CTA per SM).
 int res_smem_bytes();
 // Rows of a W-wide 2D band (core plus halo) that one CTA holds.
 int res_rows_fit2d(int W);
+// Non-empty bricks a D x H x W volume (or slab) may have to fit one CTA (0: its table does not fit).
+int res_slots_fit3d(int W, int H, int D);
 // Whether a D x H x W volume's brick table fits (its bricks are counted on the device).
 bool res_fits3d(int W, int H, int D);
 cudaError_t res_occupancy(int *per_sm);  // resident CTAs per SM

@@ -3,7 +3,8 @@
 // CTA's shared memory and thinned there from its first subiteration to its
 // fixed point; only the bands of a large image (or slabs of a large volume)
 // meet, once per iteration, to trade boundary rows through global memory.
-// One CTA of 768 threads per SM holds up to 225 KB.
+// Two CTAs of 384 threads per SM, each holding up to 111 KB, so that one
+// item's barriers do not idle the SM.
 //
 // 2D band (dense).  Rows of the band (core plus `halo` rows on each side,
 // clamped to the image) lie twice in shared memory (subiteration t reads one
@@ -47,12 +48,13 @@
 
 #include "kernels.cuh"
 #include "rules.cuh"
+#include "tiles.cuh"
 
 namespace bgt {
 
 namespace {
 constexpr int kWarps = kResThreads / 32;
-constexpr int kSmemBytes = 230400;   // dynamic shared memory per CTA
+constexpr int kSmemBytes = kResSmemBytes;  // dynamic shared memory per CTA
 constexpr int kLongAgo = -(1 << 29); // "last change" of a strip that never changed
 constexpr int kSlotWords = 129;      // 4 planes x 32 rows, plus one word so slots fall on different banks
 constexpr int kMaxBricks = 16384;    // brick table entries of a resident volume
@@ -62,27 +64,23 @@ __host__ __device__ inline size_t up16(size_t v) { return (v + 15) & ~size_t(15)
 }  // namespace
 
 // ------------------------------------------------------------ geometry ----
-__host__ __device__ inline int res_pitch2d(int W)
-{
-    const int wl = (W + 31) >> 5;
-    return 2 * ((wl + 1) >> 1) + 3;
-}
+constexpr int kUnitRowsH = 24, kUnitWordsH = 12;  // 2D unit (see the 2D section)
 
-// words of shared memory a band of nrows rows needs: zero row, two row
-// buffers and the change record of its units (at most one per 4 words of a
-// strip)
+// words of shared memory a 2D band of nrows rows needs: zero row, two row
+// copies and the activity record of its units
 __host__ __device__ inline size_t res_words2d(int W, int nrows)
 {
-    const int pp = res_pitch2d(W);
-    const int ns = (nrows + 31) >> 5;
     const int wl = (W + 31) >> 5;
-    return (size_t)pp * (1 + 2 * (size_t)nrows) + (size_t)ns * ((wl + 3) / 4);
+    const int nch = (wl + kUnitWordsH - 1) / kUnitWordsH;
+    const int pp = (nch * kUnitWordsH + 2) | 1;
+    const int ns = (nrows + kUnitRowsH - 1) / kUnitRowsH;
+    return (size_t)pp * (1 + 2 * (size_t)nrows) + (size_t)ns * nch;
 }
 
 // bytes of shared memory a volume with nb bricks of which ns are non-empty needs
 __host__ __device__ inline size_t res_bytes3d(int nb, int ns)
 {
-    return up16((size_t)nb * 2) + up16((size_t)(ns + 1) * 4) + up16((size_t)(ns + 1) * 3) +
+    return up16((size_t)nb * 2) + up16((size_t)(ns + 1) * 4) + up16((size_t)(ns + 1) * 4) +
            up16((size_t)(ns + 1) * 2) + (size_t)3 * (ns + 1) * kSlotWords * 4;
 }
 
@@ -97,6 +95,15 @@ int res_rows_fit2d(int W)
         else hi = mid - 1;
     }
     return lo;
+}
+
+int res_slots_fit3d(int W, int H, int D)
+{
+    const long long nb = (long long)((W + 31) / 32) * ((H + 31) / 32) * ((D + kBZ - 1) / kBZ);
+    if (nb > kMaxBricks) return 0;
+    int ns = 0;
+    while (res_bytes3d((int)nb, ns + 1) <= (size_t)kSmemBytes) ns++;
+    return ns;
 }
 
 bool res_fits3d(int W, int H, int D)
@@ -150,106 +157,81 @@ __device__ int res_block_exscan(int v, int *total)
 }
 
 // ------------------------------------------------------------ 2D ----------
+// A pass is one iteration (N, S, E, W) run on register tiles: a warp loads a
+// unit -- 24 core rows plus 4 halo rows above and below (lane = row) by 12
+// core words plus one halo word on either side -- from the pass-start copy,
+// runs the four subiterations in registers (run_subits2d: rows above and
+// below by shuffles, x-neighbours by funnel shifts) and writes its core to
+// the other copy.  Wrong values entering at a unit's edge move one row (or
+// bit) per subiteration, so after four they reach only its halo.
+constexpr int kUnitRows = 32 - 2 * 4;  // core rows of a unit (K = 4)
+constexpr int kUnitWords = 12;         // core words of a unit
+
+__host__ __device__ inline int res_pitch2d_tiles(int W)
+{
+    const int wl = (W + 31) >> 5;
+    const int nch = (wl + kUnitWords - 1) / kUnitWords;
+    return (nch * kUnitWords + 2) | 1;  // zero word left, zero words right, odd
+}
+
 struct Band2D {
     uint32_t *zero;     // pp zero words
-    uint32_t *buf[2];   // nrows x pp each: subiteration t reads buf[t & 1], writes buf[(t + 1) & 1]
-    int *lastchg;       // [nstrips][nchunks]: last subiteration with a deletion in the unit
-    int pp, npairs, wl, nrows, nstrips;
-    int cw, nchunks;    // words per chunk (even) and chunks per row
+    uint32_t *buf0, *buf1;  // nrows x pp each: pass q reads buf[q & 1], writes buf[(q + 1) & 1]
+    int *until;         // [nstrips][nchunks]: the unit is processed while q <= until (a unit in
+                        // its 3x3 neighbourhood deleted something in the previous pass)
+    int pp, wl, nrows, nstrips, nchunks;
     int a;              // image row of the band's first row in shared memory
     int r0, r1;         // core rows (image coordinates)
 };
 
-// Subiteration of direction DIR on words [w0, w0 + 2*np) of this lane's row
-// (w0 odd), from the pass-start rows in/up/dn to `out` (another buffer).
-// Returns the deleted bits.
-template <int DIR>
-__device__ __forceinline__ uint32_t res_row2d(const uint32_t *__restrict__ in, const uint32_t *__restrict__ up,
-                                              const uint32_t *__restrict__ dn, uint32_t *__restrict__ out,
-                                              bool store, int w0, int np)
-{
-    uint32_t ao = in[w0 - 1], bo = in[w0], au = up[w0 - 1], bu = up[w0], ad = dn[w0 - 1], bd = dn[w0];
-    uint32_t chg = 0;
-#pragma unroll 2
-    for (int k = 0; k < np; k++) {
-        const int j = w0 + 2 * k;
-        const uint32_t co = in[j + 1], eo = in[j + 2];
-        const uint32_t cu = up[j + 1], eu = up[j + 2];
-        const uint32_t cd = dn[j + 1], ed = dn[j + 2];
-        uint32_t n0 = bo, n1 = co;
-        if (__any_sync(kFull, (bo | co) != 0u)) {
-            uint32_t X[8];
-            X[0] = bu;
-            X[1] = at_xp1(bu, cu);
-            X[2] = at_xp1(bo, co);
-            X[3] = at_xp1(bd, cd);
-            X[4] = bd;
-            X[5] = at_xm1(bd, ad);
-            X[6] = at_xm1(bo, ao);
-            X[7] = at_xm1(bu, au);
-            n0 = bo & ~rule2d<DIR>(X);
-            uint32_t Y[8];
-            Y[0] = cu;
-            Y[1] = at_xp1(cu, eu);
-            Y[2] = at_xp1(co, eo);
-            Y[3] = at_xp1(cd, ed);
-            Y[4] = cd;
-            Y[5] = at_xm1(cd, bd);
-            Y[6] = at_xm1(co, bo);
-            Y[7] = at_xm1(cu, bu);
-            n1 = co & ~rule2d<DIR>(Y);
-            chg |= (n0 ^ bo) | (n1 ^ co);
-        }
-        if (store) {
-            out[j] = n0;
-            out[j + 1] = n1;
-        }
-        ao = co;
-        bo = eo;
-        au = cu;
-        bu = eu;
-        ad = cd;
-        bd = ed;
-    }
-    return chg;
-}
-
-// One subiteration t (direction DIR = t % 4) over the band's units (strip of
-// 32 rows x chunk of cw words).  A unit whose 3x3 neighbourhood of units had
-// no deletion during the last four subiterations is skipped: its
-// neighbourhood is a fixed point of the next direction, and a unit processed
-// without a change wrote identical data to both buffers.  Returns this
-// thread's deleted core bits; adds processed words to *words.
-template <int DIR>
-__device__ uint32_t res_subit2d(const Band2D &b, int t, int *take, unsigned long long *words)
+// One pass q over the band's units.  A unit whose 3x3 neighbourhood of units
+// had no deletion in the previous pass (one subiteration of every direction)
+// is skipped: that region is a fixed point, and a unit processed without a
+// change wrote identical data to both copies.  A unit that deletes something
+// extends `until` of its neighbourhood to q + 1 (a reader in the same pass
+// may see the new value: it then processes a unit it could have skipped).
+// Returns this thread's deleted core bits (band core rows only).
+__device__ uint32_t res_pass2d(const Band2D &b, int q, int *take, unsigned long long *words)
 {
     const int lane = threadIdx.x & 31;
-    const uint32_t *IN = b.buf[t & 1];
-    uint32_t *OUT = b.buf[(t + 1) & 1];
+    const uint32_t *IN = (q & 1) ? b.buf1 : b.buf0;
+    uint32_t *OUT = (q & 1) ? b.buf0 : b.buf1;
     const int nunits = b.nstrips * b.nchunks;
     uint32_t core = 0;
     for (;;) {
         const int u = res_take(take);
         if (u >= nunits) break;
+        if (b.until[u] < q) continue;
         const int s = u / b.nchunks, c = u - s * b.nchunks;
-        int lc = kLongAgo;
-        for (int ds = max(0, s - 1); ds <= min(b.nstrips - 1, s + 1); ds++)
-            for (int dc = max(0, c - 1); dc <= min(b.nchunks - 1, c + 1); dc++)
-                lc = max(lc, b.lastchg[ds * b.nchunks + dc]);
-        if (lc < t - 4) continue;
-        const int r = 32 * s + lane;
-        const bool valid = r < b.nrows;
+        const int r = kUnitRows * s - 4 + lane;
+        const bool valid = r >= 0 && r < b.nrows;
         const uint32_t *in = valid ? IN + (size_t)r * b.pp : b.zero;
-        const uint32_t *up = (r >= 1 && r - 1 < b.nrows) ? IN + (size_t)(r - 1) * b.pp : b.zero;
-        const uint32_t *dn = r + 1 < b.nrows ? IN + (size_t)(r + 1) * b.pp : b.zero;
-        uint32_t *out = OUT + (size_t)min(r, b.nrows - 1) * b.pp;
-        const int w0 = 1 + c * b.cw;
-        const int np = (min(b.cw, b.wl - c * b.cw) + 1) >> 1;
-        const uint32_t chg = res_row2d<DIR>(in, up, dn, out, valid, w0, np);
-        if (__any_sync(kFull, chg != 0u) && lane == 0) b.lastchg[u] = t;
+        const int x0 = 1 + kUnitWords * c;
+        uint32_t v[kUnitWords + 2];
+#pragma unroll
+        for (int k = 0; k < kUnitWords + 2; k++) v[k] = in[x0 - 1 + k];
+        run_subits2d<4, kUnitWords, 0>(v);
+        const bool mine = valid && lane >= 4 && lane < 4 + kUnitRows;
+        uint32_t chg = 0;
+        if (mine) {
+            uint32_t *out = OUT + (size_t)r * b.pp;
+#pragma unroll
+            for (int k = 0; k < kUnitWords; k++) {
+                chg |= v[1 + k] ^ in[x0 + k];
+                out[x0 + k] = v[1 + k];
+            }
+        }
+        if (__any_sync(kFull, chg != 0u)) {
+            if (lane < 9) {
+                const int ns = s + lane / 3 - 1, nc = c + lane % 3 - 1;
+                if (ns >= 0 && ns < b.nstrips && nc >= 0 && nc < b.nchunks) b.until[ns * b.nchunks + nc] = q + 1;
+            }
+        }
         const int gy = b.a + r;
-        if (valid && gy >= b.r0 && gy < b.r1) core |= chg;
-        if (lane == 0) *words += (unsigned long long)min(32, b.nrows - 32 * s) * min(b.cw, b.wl - c * b.cw);
+        if (mine && gy >= b.r0 && gy < b.r1) core |= chg;
+        if (lane == 0)
+            *words += (unsigned long long)min(kUnitRows, b.nrows - kUnitRows * s) *
+                      min(kUnitWords, b.wl - kUnitWords * c);
     }
     return core;
 }
@@ -260,77 +242,59 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Band2D b;
     b.wl = (in.W + 31) >> 5;
-    b.npairs = (b.wl + 1) >> 1;
-    b.pp = 2 * b.npairs + 3;
+    b.pp = res_pitch2d_tiles(in.W);
+    b.nchunks = (b.wl + kUnitWords - 1) / kUnitWords;
     b.r0 = it.r0;
     b.r1 = it.r1;
     b.a = max(0, it.r0 - it.halo);
     const int bend = min(in.H, it.r1 + it.halo);
     b.nrows = bend - b.a;
-    b.nstrips = (b.nrows + 31) >> 5;
-    // chunks: enough units per subiteration for the CTA's warps (about two
-    // each), at least 4 words (2 pairs) per chunk
-    {
-        const int want = (2 * kWarps + b.nstrips - 1) / b.nstrips;
-        int cw = (b.wl + want - 1) / want;
-        cw = max(4, (cw + 1) & ~1);
-        b.cw = cw;
-        b.nchunks = (b.wl + cw - 1) / cw;
-    }
+    b.nstrips = (b.nrows + kUnitRows - 1) / kUnitRows;
     b.zero = sm;
-    b.buf[0] = sm + b.pp;
-    b.buf[1] = b.buf[0] + (size_t)b.nrows * b.pp;
-    b.lastchg = reinterpret_cast<int *>(b.buf[1] + (size_t)b.nrows * b.pp);
+    b.buf0 = sm + b.pp;
+    b.buf1 = b.buf0 + (size_t)b.nrows * b.pp;
+    b.until = reinterpret_cast<int *>(b.buf1 + (size_t)b.nrows * b.pp);
     const int pp = b.pp;
     const int nunits = b.nstrips * b.nchunks;
 
     for (int i = threadIdx.x; i < pp; i += kResThreads) b.zero[i] = 0u;
-    for (int i = threadIdx.x; i < nunits; i += kResThreads) b.lastchg[i] = kLongAgo;
+    for (int i = threadIdx.x; i < nunits; i += kResThreads) b.until[i] = -1;
     if (threadIdx.x < 2) take[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t *g0 = in.buf[0];
     for (int r = warp; r < b.nrows; r += kWarps) {
         const uint32_t *grow = g0 + (size_t)(b.a + r) * in.P;
-        uint32_t *r0p = b.buf[0] + (size_t)r * pp, *r1p = b.buf[1] + (size_t)r * pp;
+        uint32_t *r0p = b.buf0 + (size_t)r * pp, *r1p = b.buf1 + (size_t)r * pp;
         for (int w = lane; w < pp; w += 32) {
             const uint32_t v = (w >= 1 && w <= b.wl) ? __ldcg(grow + (w - 1)) : 0u;
             r0p[w] = v;
             r1p[w] = v;
-            // units holding foreground start as "changed just before t = 0"
-            if (v && w <= b.wl) b.lastchg[(r >> 5) * b.nchunks + (w - 1) / b.cw] = -1;
+            // units holding foreground start active
+            if (v) b.until[(r / kUnitRows) * b.nchunks + (w - 1) / kUnitWords] = 0;
         }
     }
     __syncthreads();
 
-    int last_any = -1;  // last subiteration with a core deletion (same in every thread)
-    int result = 0;     // 1 converged, -1 pass cap or failed wait
+    int result = 0;  // 1 converged, -1 pass cap or failed wait
     unsigned long long words = 0;
-    const int cap_t = 4 * in.pass_cap;
-    int t = 0;
-    for (;; t++) {
-        // the counter of this subiteration was cleared during the previous
-        // one; clear the next one's (nobody uses it before the barrier below)
-        if (threadIdx.x == 0) take[(t + 1) & 1] = 0;
-        uint32_t core;
-        switch (t & 3) {
-        case 0: core = res_subit2d<0>(b, t, take + (t & 1), &words); break;
-        case 1: core = res_subit2d<1>(b, t, take + (t & 1), &words); break;
-        case 2: core = res_subit2d<2>(b, t, take + (t & 1), &words); break;
-        default: core = res_subit2d<3>(b, t, take + (t & 1), &words); break;
-        }
-        if (__syncthreads_or(core != 0u)) last_any = t;
+    int q = 0;
+    for (;; q++) {
+        // the counter of this pass was cleared during the previous one;
+        // clear the next one's (nobody uses it before the barrier below)
+        if (threadIdx.x == 0) take[(q + 1) & 1] = 0;
+        const uint32_t core = res_pass2d(b, q, take + (q & 1), &words);
+        const bool any = __syncthreads_or(core != 0u);
         if (it.bands == 1) {
-            if (t - last_any >= 4) {
+            if (!any) {
                 result = 1;
                 break;
             }
-        } else if ((t & 3) == 3) {
-            // end of iteration p (state in buf[(t+1)&1]): trade boundary rows
-            // with the neighbouring bands
-            const int p = t >> 2;
+        } else {
+            // end of pass q (state in buf[(q+1)&1]): trade boundary rows with
+            // the neighbouring bands
             const int h = it.halo;
-            uint32_t *cur = b.buf[(t + 1) & 1];
-            uint32_t *gx = in.buf[(p + 1) & 1];  // buf[0] holds the start state other bands may still load
+            uint32_t *cur = (q & 1) ? b.buf0 : b.buf1;
+            uint32_t *gx = in.buf[(q + 1) & 1];  // buf[0] holds the start state other bands may still load
             for (int k = warp; k < 2 * h; k += kWarps) {
                 const bool top = k < h;
                 if (top ? it.band == 0 : it.band + 1 == it.bands) continue;
@@ -342,14 +306,14 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
-                if (last_any >= 4 * p) atomicMax(&in.res_last, p);
+                if (any) atomicMax(&in.res_last, q);
                 atomicAdd(&in.res_arrive, 1);
                 int f;
-                if (!res_wait_at_least(&in.res_arrive, it.bands * (p + 1), S->timeout_ns)) {
+                if (!res_wait_at_least(&in.res_arrive, it.bands * (q + 1), S->timeout_ns)) {
                     atomicOr(&S->status, kErrQueueTimeout);
                     f = 2;
                 } else {
-                    f = ld_acquire(&in.res_last) < p ? 1 : 0;
+                    f = ld_acquire(&in.res_last) < q ? 1 : 0;
                 }
                 s_flag = f;
             }
@@ -363,7 +327,7 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
                 result = -1;
                 break;
             }
-            // halo rows: the neighbours' boundary core rows after iteration p
+            // halo rows: the neighbours' boundary core rows after pass q
             const int ntop = b.r0 - b.a, nh = ntop + (bend - b.r1);
             uint32_t hc = 0;
             for (int k = warp; k < nh; k += kWarps) {
@@ -377,33 +341,33 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
                 }
             }
             if (__syncthreads_or(hc != 0u)) {
-                // the units holding halo rows changed
+                // units within reach of the halo rows go on next pass
                 for (int u = threadIdx.x; u < nunits; u += kResThreads) {
                     const int st = u / b.nchunks;
-                    const int ga = b.a + 32 * st, gb = b.a + min(32 * st + 32, b.nrows);
-                    if (ga < b.r0 || gb > b.r1) b.lastchg[u] = t;
+                    const int ga = b.a + kUnitRows * st - kUnitRows, gb = b.a + kUnitRows * st + 2 * kUnitRows;
+                    if (ga < b.r0 || gb > b.r1) b.until[u] = q + 1;
                 }
                 __syncthreads();
             }
         }
-        if (t >= cap_t) {
+        if (q >= in.pass_cap) {
             if (threadIdx.x == 0) atomicOr(&S->status, kErrPassLimit);
             result = -1;
             break;
         }
     }
-    // the converged core rows (in buf[(t+1)&1]) -> buf[0]
+    // the converged core rows (in buf[(q+1)&1]) -> buf[0]
     __syncthreads();
-    const uint32_t *fin = b.buf[(t + 1) & 1];
+    const uint32_t *fin = (q & 1) ? b.buf0 : b.buf1;
     uint32_t *g0w = in.buf[0];
     for (int r = b.r0 - b.a + warp; r < b.r1 - b.a; r += kWarps) {
         const uint32_t *srow = fin + (size_t)r * pp;
         uint32_t *grow = g0w + (size_t)(b.a + r) * in.P;
         for (int w = lane; w < b.wl; w += 32) grow[w] = srow[w + 1];
     }
-    if (lane == 0 && words) atomicAdd(&in.work_words, words / 4);  // one pass = one iteration of 4 subiterations
+    if (lane == 0 && words) atomicAdd(&in.work_words, words);  // core words per pass (one iteration)
     if (threadIdx.x == 0) {
-        if (it.band == 0) in.passes_run = (t + 4) / 4;
+        if (it.band == 0) in.passes_run = q + 1;
         if (result < 0) atomicMin(&in.converged, -1);
         atomicAdd(&in.tiles_run, 1ull);
     }
@@ -417,6 +381,7 @@ struct Vol3D {
     uint8_t *act;      // slot: active in this iteration
     uint8_t *chg;      // slot: changed in this iteration
     uint8_t *nxt;      // slot: active in the next iteration
+    uint8_t *ufl;      // slot: its pre-test union of this iteration is not empty
     uint16_t *list;    // active slots of this iteration
     uint32_t *X, *Y, *U;  // slot buffers (slot 0 = the zero brick)
     int nbx, nby, nbz, nslots;
@@ -425,7 +390,7 @@ struct Vol3D {
 // The nine row/word neighbourhood words of one plane (offset `off` within
 // the slots) from the slot bases of the rows above (u), this row (o) and
 // below (d), each for the words x-1, x, x+1.
-__device__ __forceinline__ void res_plane9(const uint32_t *IN, const int (&u)[3], const int (&o)[3],
+__device__ __forceinline__ void res_plane9(const uint32_t *__restrict__ IN, const int (&u)[3], const int (&o)[3],
                                            const int (&d)[3], int off, uint32_t (&P)[9])
 {
     const uint32_t ul = IN[u[0] + off], uc = IN[u[1] + off], ur = IN[u[2] + off];
@@ -455,8 +420,10 @@ __device__ __forceinline__ void res_bases3d(int nb27, int dzb, int (&u)[3], int 
 }
 
 // Subiteration J (0: pre-test union + U; 1..5: N, E, D, S, W) on brick slot s.
+// J = 0 also ORs the brick's union bits into *uany.
 template <int J>
-__device__ uint32_t res_brick3d(const Vol3D &v, int s, const uint32_t *IN, uint32_t *OUT, uint32_t *U)
+__device__ uint32_t res_brick3d(const Vol3D &v, int s, const uint32_t *__restrict__ IN, uint32_t *__restrict__ OUT,
+                                uint32_t *__restrict__ U, uint32_t *uany)
 {
     const int lane = threadIdx.x & 31;
     const int li = v.coord[s];
@@ -497,6 +464,7 @@ __device__ uint32_t res_brick3d(const Vol3D &v, int s, const uint32_t *IN, uint3
                 nv = val & ~du;
             }
             U[widx] = un;
+            *uany |= un;
         } else {
             const uint32_t cand = val & U[widx];
             if (__any_sync(kFull, cand != 0u)) {
@@ -607,7 +575,8 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
     v.act = smb + off;
     v.chg = v.act + (total + 1);
     v.nxt = v.chg + (total + 1);
-    off += up16((size_t)(total + 1) * 3);
+    v.ufl = v.nxt + (total + 1);
+    off += up16((size_t)(total + 1) * 4);
     v.list = reinterpret_cast<uint16_t *>(smb + off);
     off += up16((size_t)(total + 1) * 2);
     v.X = reinterpret_cast<uint32_t *>(smb + off);
@@ -631,6 +600,7 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
         v.act[i] = i > 0;
         v.chg[i] = 0;
         v.nxt[i] = 0;
+        v.ufl[i] = 0;
     }
     if (threadIdx.x < 2) take[threadIdx.x] = 0;
     __syncthreads();
@@ -676,8 +646,19 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
         for (int s = threadIdx.x + 1; s <= total; s += kResThreads)
             if (v.act[s]) v.list[atomicAdd(&s_cnt, 1)] = (uint16_t)s;
         __syncthreads();
-        const int nact = s_cnt;
+        int nact = s_cnt;
         for (int j = 0; j < 6; j++) {
+            if (j == 1) {
+                // a brick whose union is empty cannot change in the rest of
+                // the iteration (every deletion is of a union voxel), and both
+                // of its buffers already hold its state: only the others go on
+                if (threadIdx.x == 0) s_cnt = 0;
+                __syncthreads();
+                for (int s = threadIdx.x + 1; s <= total; s += kResThreads)
+                    if (v.act[s] && v.ufl[s]) v.list[atomicAdd(&s_cnt, 1)] = (uint16_t)s;
+                __syncthreads();
+                nact = s_cnt;
+            }
             if (threadIdx.x == 0) take[(j + 1) & 1] = 0;
             const uint32_t *IN = (j & 1) ? v.Y : v.X;
             uint32_t *OUT = (j & 1) ? v.X : v.Y;
@@ -685,14 +666,18 @@ __device__ void res_run3d(Inst &in, const ResItem &it, uint8_t *smb, ResSched *S
                 const int k = res_take(take + (j & 1));
                 if (k >= nact) break;
                 const int s = v.list[k];
-                uint32_t c;
+                uint32_t c, uany = 0;
                 switch (j) {
-                case 0: c = res_brick3d<0>(v, s, IN, OUT, v.U); break;
-                case 1: c = res_brick3d<1>(v, s, IN, OUT, v.U); break;
-                case 2: c = res_brick3d<2>(v, s, IN, OUT, v.U); break;
-                case 3: c = res_brick3d<3>(v, s, IN, OUT, v.U); break;
-                case 4: c = res_brick3d<4>(v, s, IN, OUT, v.U); break;
-                default: c = res_brick3d<5>(v, s, IN, OUT, v.U); break;
+                case 0: c = res_brick3d<0>(v, s, IN, OUT, v.U, &uany); break;
+                case 1: c = res_brick3d<1>(v, s, IN, OUT, v.U, &uany); break;
+                case 2: c = res_brick3d<2>(v, s, IN, OUT, v.U, &uany); break;
+                case 3: c = res_brick3d<3>(v, s, IN, OUT, v.U, &uany); break;
+                case 4: c = res_brick3d<4>(v, s, IN, OUT, v.U, &uany); break;
+                default: c = res_brick3d<5>(v, s, IN, OUT, v.U, &uany); break;
+                }
+                if (j == 0) {
+                    const bool u = __any_sync(kFull, uany != 0u);
+                    if (lane == 0) v.ufl[s] = u;
                 }
                 if (lane == 0) {
                     const int li = v.coord[s];
@@ -834,7 +819,7 @@ __device__ __forceinline__ int res_smid()
     return v;
 }
 
-__global__ void __launch_bounds__(kResThreads, 1)
+__global__ void __launch_bounds__(kResThreads, kResCtasPerSm)
     resident_kernel(Inst *insts, const ResItem *items, ResSched *S, ResTrace *trace)
 {
     extern __shared__ __align__(16) uint8_t res_smem[];
@@ -860,6 +845,8 @@ __global__ void __launch_bounds__(kResThreads, 1)
 cudaError_t res_occupancy(int *per_sm)
 {
     cudaError_t e = cudaFuncSetAttribute(resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(resident_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, resident_kernel, kResThreads, kSmemBytes);
 }
@@ -870,6 +857,8 @@ cudaError_t launch_resident(int grid, Inst *d_insts, int ninst, const ResItem *d
     static bool attr_done = false;
     if (!attr_done) {
         cudaError_t e = cudaFuncSetAttribute(resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(resident_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
         attr_done = true;
     }
