@@ -184,12 +184,14 @@ struct Band2D {
     int r0, r1;         // core rows (image coordinates)
 };
 
-// One pass q over the band's units.  A unit whose 3x3 neighbourhood of units
-// had no deletion in the previous pass (one subiteration of every direction)
-// is skipped: that region is a fixed point, and a unit processed without a
+// One pass q over the band's units.  A unit none of whose inputs for the
+// pass -- its core and the 4-pixel border bands of its 3x3 neighbours -- had
+// a deletion in the previous pass (one subiteration of every direction) is
+// skipped: that region is a fixed point, and a unit processed without a
 // change wrote identical data to both copies.  A unit that deletes something
-// extends `until` of its neighbourhood to q + 1 (a reader in the same pass
-// may see the new value: it then processes a unit it could have skipped).
+// extends `until` to q + 1 for itself and for each neighbour whose border
+// band the deletions reach (a reader in the same pass may see the new value:
+// it then processes a unit it could have skipped).
 // Returns this thread's deleted core bits (band core rows only).
 __device__ uint32_t res_pass2d(const Band2D &b, int q, int *take, unsigned long long *words)
 {
@@ -212,21 +214,36 @@ __device__ uint32_t res_pass2d(const Band2D &b, int q, int *take, unsigned long 
         for (int k = 0; k < kUnitWords + 2; k++) v[k] = in[x0 - 1 + k];
         run_subits2d<4, kUnitWords, 0>(v);
         const bool mine = valid && lane >= 4 && lane < 4 + kUnitRows;
-        uint32_t chg = 0;
+        uint32_t chg = 0, lft = 0, rgt = 0;
         if (mine) {
             uint32_t *out = OUT + (size_t)r * b.pp;
 #pragma unroll
             for (int k = 0; k < kUnitWords; k++) {
-                chg |= v[1 + k] ^ in[x0 + k];
+                const uint32_t d = v[1 + k] ^ in[x0 + k];
+                chg |= d;
+                if (k == 0) lft = d & 0xFu;                     // within 4 pixels of the left edge
+                if (k == kUnitWords - 1) rgt = d & 0xF0000000u;  // ... of the right edge
                 out[x0 + k] = v[1 + k];
             }
         }
-        if (__any_sync(kFull, chg != 0u)) {
+        // The next pass of a neighbour depends on this unit only through the
+        // 4 pixels next to their common border (four subiterations reach 4
+        // pixels): activate the neighbours whose border band changed
+        // (border bands, as the tile engine does).
+        const unsigned m_any = __ballot_sync(kFull, chg != 0u);
+        if (m_any) {
+            const unsigned m_l = __ballot_sync(kFull, lft != 0u), m_r = __ballot_sync(kFull, rgt != 0u);
+            const unsigned band_top = 0x000000F0u, band_bot = 0x0F000000u;  // lanes 4..7, 24..27
             if (lane < 9) {
-                const int ns = s + lane / 3 - 1, nc = c + lane % 3 - 1;
-                if (ns >= 0 && ns < b.nstrips && nc >= 0 && nc < b.nchunks) b.until[ns * b.nchunks + nc] = q + 1;
+                const int dy = lane / 3 - 1, dx = lane % 3 - 1;
+                const unsigned rows = dy < 0 ? band_top : dy > 0 ? band_bot : ~0u;
+                const unsigned cols = dx < 0 ? m_l : dx > 0 ? m_r : m_any;
+                const int ns = s + dy, nc = c + dx;
+                if ((rows & cols & m_any) && ns >= 0 && ns < b.nstrips && nc >= 0 && nc < b.nchunks)
+                    b.until[ns * b.nchunks + nc] = q + 1;
             }
         }
+
         const int gy = b.a + r;
         if (mine && gy >= b.r0 && gy < b.r1) core |= chg;
         if (lane == 0)

@@ -2,9 +2,9 @@
 (begputhinning_b200/csrc/resident.cu: res_run2d, res_pass2d): an image cut
 into bands of rows that each keep `halo` extra rows on both sides; a pass is
 one iteration (N, S, E, W) computed per unit of 24 rows x 12 words on a
-register tile with 4 halo rows and one halo word on either side; units are
-skipped while no unit of their 3x3 neighbourhood changed in the previous
-pass; the bands run passes in lockstep with a halo exchange after each, and
+register tile with 4 halo rows and one halo word on either side; a unit is
+processed in the next pass when it changed or a neighbour changed within 4
+pixels of their common border (border bands); the bands run passes in lockstep with a halo exchange after each, and
 stop after a pass without a core deletion in any band.
 Deletions use the oracle's rule table, so the model checks the protocol and
 its exactness argument, not the device's arithmetic: it must reproduce the
@@ -89,10 +89,22 @@ def run_band_model(img, bands, halo=4, unit_rows=24, unit_px=12 * 32):
                     y0, y1 = unit_rows * s, min(unit_rows * (s + 1), rows.shape[0])
                     x0, x1 = unit_px * c, min(unit_px * (c + 1), W)
                     out = run_tile(rows, y0, y1, x0, x1)
-                    if (out != rows[y0:y1, x0:x1]).any():
-                        until[max(0, s - 1):s + 2, max(0, c - 1):c + 2] = q + 1
+                    d = out != rows[y0:y1, x0:x1]
+                    if d.any():
+                        # border bands: a neighbour is activated only when a
+                        # change lies within 4 pixels of its side
+                        band_r = {-1: d[:4].any(axis=0), 0: d.any(axis=0), 1: d[unit_rows - 4:].any(axis=0)}
+                        for dy in (-1, 0, 1):
+                            if dy == 1 and y1 - y0 < unit_rows:
+                                continue  # last unit of the band: no unit below
+                            rr = band_r[dy]
+                            for dx in (-1, 0, 1):
+                                hit = rr[:4].any() if dx < 0 else rr[-4:].any() if dx > 0 else rr.any()
+                                ns, nc = s + dy, c + dx
+                                if hit and 0 <= ns < until.shape[0] and 0 <= nc < nch:
+                                    until[ns, nc] = q + 1
                         ga, gb = bd["a"] + y0, bd["a"] + y1
-                        ch = (out != rows[y0:y1, x0:x1]).any(axis=1)
+                        ch = d.any(axis=1)
                         ys = np.arange(ga, gb)[ch]
                         any_core |= bool(((ys >= bd["r0"]) & (ys < bd["r1"])).any())
                     new[y0:y1, x0:x1] = out
