@@ -68,9 +68,9 @@ struct ResTrace {
     long long t0, t1;
     int sm, pad;
 };
-constexpr int kResThreads = 384;
-constexpr int kResCtasPerSm = 2;
-constexpr int kResSmemBytes = 113664;  // dynamic shared memory of one CTA (two per SM)
+constexpr int kResThreads = 768;
+constexpr int kResCtasPerSm = 1;
+constexpr int kResSmemBytes = 230400;  // dynamic shared memory of one CTA (one per SM)
 // Dynamic shared memory of the resident kernel (one CTA per SM).
 int res_smem_bytes();
 // Rows of a W-wide 2D band (core plus halo) that one CTA holds.

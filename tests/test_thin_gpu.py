@@ -227,3 +227,32 @@ def test_engine_small_grids_and_gangs(ctx, ctas):
             assert np.array_equal(o.cpu().numpy(), want), f"instance {k}, run {rep}"
             assert b.stats(ids[k])["converged"] == 1
     b.close()
+
+
+def test_vessels_4096_full_size(ctx):
+    """The 4096 x 4096 vessel-tree image (20 roots, branching depth 6, 0.1%
+    salt, 50 holes) at full size -- the width at which the reference's own
+    Thinning2D divides by zero (2D/LibThinning2D.cu:63-67) -- thinned
+    through the host API and as a one-instance batch on the tile rings."""
+    from begputhinning_b200 import Thinning2D, synth
+    img = synth.vessels4096(1)
+    want = po.thin2d(img)[0]
+    got = Thinning2D(img, ctx)
+    assert np.array_equal(got, want), f"{(got != want).sum()} px differ"
+    (ring,), _ = _run_batch(ctx, [img], 2, False)
+    assert np.array_equal(ring, want)
+
+
+def test_benchmark_subset_with_wide_images(ctx):
+    """The first 160 images of the benchmark batch's generator -- 26 of them
+    1025-2048 pixels wide -- and four tree volumes, thinned together in one
+    batch (the wide images are the ones cut into bands)."""
+    from begputhinning_b200 import synth
+    imgs, vols = synth.mixed_batch(3, 160, 4)
+    assert sum(1 for im in imgs if im.shape[1] > 1024) == 26
+    items = imgs + vols
+    got, stats = _run_batch(ctx, items, -1, False)
+    for k, (g, it) in enumerate(zip(got, items)):
+        want = po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0]
+        assert np.array_equal(g, want), f"instance {k} shape {it.shape}"
+    assert all(s["converged"] == 1 for s in stats)
