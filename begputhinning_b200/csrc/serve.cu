@@ -122,6 +122,19 @@ struct Arena {
 
 size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 
+// Host<->device copy in pieces of at most 4 MB, so that the copies of other
+// slots (frames on high-priority streams) interleave with a large volume's
+// instead of queueing behind all of it.
+cudaError_t copy_pieces(void *dst, const void *src, size_t n, cudaMemcpyKind kind, cudaStream_t st)
+{
+    constexpr size_t kPiece = size_t(4) << 20;
+    cudaError_t e = cudaSuccess;
+    for (size_t o = 0; o < n && e == cudaSuccess; o += kPiece)
+        e = cudaMemcpyAsync(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, std::min(kPiece, n - o),
+                            kind, st);
+    return e;
+}
+
 // Arena bytes of one launch of these requests: staging (inputs and
 // outputs) plus the batch pool their shapes need.
 size_t launch_bytes(const std::vector<Req *> &reqs, int cfg)
@@ -183,8 +196,7 @@ int launch_slot(bgt_server *S, Slot &s)
     if (rc != BGT_OK) return rc;
     cudaError_t e = cudaSuccess;
     for (size_t i = 0; i < s.reqs.size() && e == cudaSuccess; i++)
-        e = cudaMemcpyAsync(blk + in_off[i], s.reqs[i]->host_in, s.reqs[i]->bytes, cudaMemcpyHostToDevice,
-                            s.stream);
+        e = copy_pieces(blk + in_off[i], s.reqs[i]->host_in, s.reqs[i]->bytes, cudaMemcpyHostToDevice, s.stream);
     if (e != cudaSuccess) return cuda_fail(e, "serve H2D");
     for (size_t i = 0; i < s.reqs.size() && rc == BGT_OK; i++) {
         const Req *r = s.reqs[i];
@@ -197,8 +209,7 @@ int launch_slot(bgt_server *S, Slot &s)
     if (rc == BGT_OK) rc = bgt_batch_run(b, 0, 0);
     if (rc != BGT_OK) return rc;
     for (size_t i = 0; i < s.reqs.size() && e == cudaSuccess; i++)
-        e = cudaMemcpyAsync(s.reqs[i]->host_out, blk + out_off[i], s.reqs[i]->bytes, cudaMemcpyDeviceToHost,
-                            s.stream);
+        e = copy_pieces(s.reqs[i]->host_out, blk + out_off[i], s.reqs[i]->bytes, cudaMemcpyDeviceToHost, s.stream);
     if (e == cudaSuccess) e = cudaEventRecord(s.done, s.stream);
     if (e != cudaSuccess) return cuda_fail(e, "serve D2H");
     (void)S;
@@ -213,6 +224,8 @@ void dispatcher_loop(bgt_server *S)
         bool launched = false;
         for (int li = 0; li < 2; li++) {
             Lane &L = S->lane[li];
+            // frames first: no volume is admitted while a frame waits
+            if (li == 1 && !S->lane[0].pending.empty()) continue;
             for (Slot &s : L.slots) {
                 if (s.busy || L.pending.empty()) continue;
                 // admit from the front while the lane's share and the arena
