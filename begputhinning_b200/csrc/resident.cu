@@ -55,7 +55,6 @@ namespace bgt {
 namespace {
 constexpr int kWarps = kResThreads / 32;
 constexpr int kSmemBytes = kResSmemBytes;  // dynamic shared memory per CTA
-constexpr int kLongAgo = -(1 << 29); // "last change" of a strip that never changed
 constexpr int kSlotWords = 129;      // 4 planes x 32 rows, plus one word so slots fall on different banks
 constexpr int kMaxBricks = 16384;    // brick table entries of a resident volume
 constexpr int kBZ = 4;               // planes per brick
