@@ -63,7 +63,7 @@ __host__ __device__ inline size_t up16(size_t v) { return (v + 15) & ~size_t(15)
 }  // namespace
 
 // ------------------------------------------------------------ geometry ----
-constexpr int kUnitRowsH = 24, kUnitWordsH = 12;  // 2D unit (see the 2D section)
+constexpr int kUnitRowsH = 24, kUnitWordsH = 8;  // 2D unit (see the 2D section)
 
 // words of shared memory a 2D band of nrows rows needs: zero row, two row
 // copies and the activity record of its units
@@ -157,14 +157,14 @@ __device__ int res_block_exscan(int v, int *total)
 
 // ------------------------------------------------------------ 2D ----------
 // A pass is one iteration (N, S, E, W) run on register tiles: a warp loads a
-// unit -- 24 core rows plus 4 halo rows above and below (lane = row) by 12
+// unit -- 24 core rows plus 4 halo rows above and below (lane = row) by 8
 // core words plus one halo word on either side -- from the pass-start copy,
 // runs the four subiterations in registers (run_subits2d: rows above and
 // below by shuffles, x-neighbours by funnel shifts) and writes its core to
 // the other copy.  Wrong values entering at a unit's edge move one row (or
 // bit) per subiteration, so after four they reach only its halo.
 constexpr int kUnitRows = 32 - 2 * 4;  // core rows of a unit (K = 4)
-constexpr int kUnitWords = 12;         // core words of a unit
+constexpr int kUnitWords = 8;          // core words of a unit
 
 __host__ __device__ inline int res_pitch2d_tiles(int W)
 {

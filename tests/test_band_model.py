@@ -1,7 +1,7 @@
 """A CPU model of the resident kernel's 2D protocol
 (begputhinning_b200/csrc/resident.cu: res_run2d, res_pass2d): an image cut
 into bands of rows that each keep `halo` extra rows on both sides; a pass is
-one iteration (N, S, E, W) computed per unit of 24 rows x 12 words on a
+one iteration (N, S, E, W) computed per unit of 24 rows x 8 words on a
 register tile with 4 halo rows and one halo word on either side; a unit is
 processed in the next pass when it changed or a neighbour changed within 4
 pixels of their common border (border bands); the bands run passes in lockstep with a halo exchange after each, and
@@ -58,7 +58,7 @@ def run_tile(rows, r0, r1, c0, c1):
     return t[4:4 + (r1 - r0), 32:32 + (c1 - c0)]
 
 
-def run_band_model(img, bands, halo=4, unit_rows=24, unit_px=12 * 32):
+def run_band_model(img, bands, halo=4, unit_rows=24, unit_px=8 * 32):
     H, W = img.shape
     state = img.copy()  # global buffer (the bands' boundary rows are traded through it)
     cuts = [k * H // bands for k in range(bands + 1)]
