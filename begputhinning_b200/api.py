@@ -297,14 +297,19 @@ class Batch:
         check(lib().bgt_batch_set_io(self.h, i, torch_dtype_code(t_in), t_in.data_ptr(),
                                      t_out.data_ptr() if t_out is not None else None))
 
-    def run(self, plain: bool = False, graph: bool = True, sync: bool = True) -> None:
+    def run(self, plain: bool = False, graph: bool = True, sync: bool = True, device_loop: bool = False) -> None:
         """Run the batch on the context's stream.  With sync (default) the
         caller's torch stream is drained first and the device is synchronised
-        after, so torch tensors can be used directly before and after."""
+        after, so torch tensors can be used directly before and after.
+        `plain` runs one launch per pass per instance; with `device_loop` the
+        pass loop of the plain path stays on the device (a CUDA graph with a
+        conditional node per instance) instead of reading the change flag
+        back after every pass."""
         if sync:
             import torch
             torch.cuda.current_stream().synchronize()
-        check(lib().bgt_batch_run(self.h, 1 if plain else 0, 0 if plain else int(graph)))
+        mode = (2 if device_loop else 1) if plain else 0
+        check(lib().bgt_batch_run(self.h, mode, 0 if plain else int(graph)))
         if sync:
             import torch
             torch.cuda.synchronize()

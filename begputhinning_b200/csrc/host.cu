@@ -90,7 +90,7 @@ extern "C" int bgt_ctx_set_stream(bgt_ctx *c, void *stream)
 {
     if (!c) return fail(BGT_ERR_ARG, "null context");
     c->stream = stream ? (cudaStream_t)stream : c->own;
-    for (auto &kv : c->cache) kv.second->graph_valid = false;
+    for (auto &kv : c->cache) kv.second->graph_valid = kv.second->pgraph_valid = false;
     return BGT_OK;
 }
 
@@ -181,9 +181,13 @@ static void batch_free_device(bgt_batch *b)
         }
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;
-    b->graph_valid = false;
+    if (b->pexec) cudaGraphExecDestroy(b->pexec);
+    b->pexec = nullptr;
+    b->graph_valid = b->pgraph_valid = false;
     if (b->pool && !b->external) cudaFree(b->pool);
     b->pool = nullptr;
+    if (b->d_ploop) cudaFree(b->d_ploop);
+    b->d_ploop = nullptr;
 }
 
 int bgt::batch_use_pool(bgt_batch *b, void *pool, size_t bytes)
@@ -562,7 +566,11 @@ extern "C" int bgt_batch_reset(bgt_batch *b)
     }
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;
-    b->graph_valid = false;
+    if (b->pexec) cudaGraphExecDestroy(b->pexec);
+    b->pexec = nullptr;
+    if (b->d_ploop) cudaFree(b->d_ploop);  // sized for the old instance count
+    b->d_ploop = nullptr;
+    b->graph_valid = b->pgraph_valid = false;
     b->items.clear();
     b->h.clear();
     b->io.clear();
@@ -676,7 +684,7 @@ extern "C" int bgt_batch_set_io(bgt_batch *b, int id, int dtype, const void *d_i
     if (dtype_size(dtype) == 0) return fail(BGT_ERR_ARG, "bad dtype %d", dtype);
     IO &io = b->io[id];
     if (io.in != d_in || io.out != d_out || io.dtype != dtype) {
-        b->graph_valid = false;
+        b->graph_valid = b->pgraph_valid = false;
         b->io_dirty = true;
     }
     io.dtype = dtype;
@@ -692,7 +700,7 @@ int bgt::batch_set_input_extent(bgt_batch *b, int id, int inW, int inH, int inD)
     if (inW > in.W || inH > in.H || inD > in.D) return fail(BGT_ERR_ARG, "input extent larger than the instance");
     IO &io = b->io[id];
     if (io.inW != inW || io.inH != inH || io.inD != inD) {
-        b->graph_valid = false;
+        b->graph_valid = b->pgraph_valid = false;
         b->io_dirty = true;
     }
     io.inW = inW;
@@ -915,11 +923,119 @@ static int run_plain(bgt_batch *b)
     return rc;
 }
 
+// The plain path with its pass loop on the device: one CUDA graph for the
+// batch in which every instance is packed, thinned by a conditional WHILE
+// node (body: one pass over all its tiles, then plain_loop_step_kernel, which
+// applies run_plain's convergence rule and sets the condition), and
+// unpacked, one instance after another.  No pass waits for the host.
+static int capture_into(cudaGraph_t g, cudaStream_t st, const cudaGraphNode_t *deps, size_t ndeps)
+{
+    cudaError_t e = cudaStreamBeginCaptureToGraph(st, g, deps, nullptr, ndeps, cudaStreamCaptureModeThreadLocal);
+    return e == cudaSuccess ? BGT_OK : cuda_fail(e, "cudaStreamBeginCaptureToGraph");
+}
+
+static int capture_tail(cudaStream_t st, std::vector<cudaGraphNode_t> &tail)
+{
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *d = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &d, &nd);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamGetCaptureInfo");
+    tail.assign(d, d + nd);
+    return BGT_OK;
+}
+
+static int build_plain_graph(bgt_batch *b, cudaGraph_t g)
+{
+    cudaStream_t st = b->ctx->stream;
+    const int N = (int)b->items.size();
+    int *d_err = &b->d_sched->status;
+    std::vector<cudaGraphNode_t> tail;
+    cudaGraph_t dummy = nullptr;
+    int rc = capture_into(g, st, nullptr, 0);
+    if (rc != BGT_OK) return rc;
+    cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(int), st);
+    for (int i = 0; i < N && e == cudaSuccess; i++) {
+        const Inst &in = b->h[i];
+        const IO &io = b->io[i];
+        if (!io.in) {
+            cudaStreamEndCapture(st, &dummy);
+            return fail(BGT_ERR_STATE, "instance %d has no input", i);
+        }
+        e = launch_pack(io.dtype, in.dims == 2 ? 0 : 1, io.in, io.inW ? io.inW : in.W, io.inH ? io.inH : in.H,
+                        io.inD ? io.inD : in.D, in.W, in.H, in.D, in.P, in.buf[0], in.buf[1], st);
+        if (e == cudaSuccess) e = launch_tile_init(b->d_insts + i, in, nullptr, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(&b->d_insts[i].tiles_run, 0, 2 * sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = launch_plain_loop_init(b->d_ploop + i, st);
+        if (e != cudaSuccess) break;
+        rc = capture_tail(st, tail);
+        cudaStreamEndCapture(st, &dummy);
+        if (rc != BGT_OK) return rc;
+        cudaGraphConditionalHandle h;
+        e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphConditionalHandleCreate");
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cn;
+        e = cudaGraphAddNode(&cn, g, tail.data(), tail.size(), &cp);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphAddNode (while)");
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        rc = capture_into(body, st, nullptr, 0);
+        if (rc != BGT_OK) return rc;
+        e = launch_plain_dev_pass(in.cfg, b->d_insts + i, in.ntiles, b->d_ploop + i, d_err, st);
+        if (e == cudaSuccess) e = launch_plain_loop_step(b->d_ploop + i, b->d_insts + i, d_err, h, st);
+        cudaStreamEndCapture(st, &dummy);
+        if (e != cudaSuccess) return cuda_fail(e, "plain pass (capture)");
+        rc = capture_into(g, st, &cn, 1);
+        if (rc != BGT_OK) return rc;
+        if (io.out) e = launch_unpack(io.dtype, in.buf[0], in.W, in.H, in.D, in.P, io.out, st);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(st, &dummy);
+    if (e != cudaSuccess) return cuda_fail(e, "plain graph");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    return BGT_OK;
+}
+
+static int run_plain_device(bgt_batch *b)
+{
+    cudaStream_t st = b->ctx->stream;
+    const int N = (int)b->items.size();
+    if (N == 0) return BGT_OK;
+    if (!b->d_ploop) {
+        cudaError_t e = cudaMalloc(&b->d_ploop, sizeof(PlainLoop) * (size_t)N);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (plain loop state)");
+    }
+    if (!b->pgraph_valid) {
+        if (b->pexec) cudaGraphExecDestroy(b->pexec);
+        b->pexec = nullptr;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaGraphCreate(&g, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphCreate");
+        int rc = build_plain_graph(b, g);
+        if (rc == BGT_OK) {
+            e = cudaGraphInstantiate(&b->pexec, g, 0);
+            if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate (plain)");
+        }
+        cudaGraphDestroy(g);
+        if (rc != BGT_OK) return rc;
+        b->pgraph_valid = true;
+    }
+    cudaError_t e = cudaGraphLaunch(b->pexec, st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch (plain)");
+    b->stats_valid = false;
+    b->last_mode = 2;
+    return BGT_OK;
+}
+
 extern "C" int bgt_batch_run(bgt_batch *b, int mode, int use_graph)
 {
     if (!b || !b->finalized) return fail(BGT_ERR_STATE, "batch not finalized");
+    if (mode < 0 || mode > 2) return fail(BGT_ERR_ARG, "mode must be 0 (engine), 1 (plain) or 2 (plain, device loop)");
     cudaSetDevice(b->ctx->device);
-    int rc = mode == 1 ? run_plain(b) : run_engine(b, use_graph);
+    int rc = mode == 1 ? run_plain(b) : mode == 2 ? run_plain_device(b) : run_engine(b, use_graph);
     if (rc != BGT_OK) return rc;
     return BGT_OK;
 }

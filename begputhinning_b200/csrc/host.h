@@ -132,4 +132,8 @@ struct bgt_batch {
     bool any_res3d = false;           // some volume may spill from the resident engine to the rings
     cudaGraphExec_t gexec = nullptr;
     bool graph_valid = false;
+    // plain path with the pass loop on the device (bgt_batch_run mode 2)
+    cudaGraphExec_t pexec = nullptr;
+    bool pgraph_valid = false;
+    bgt::PlainLoop *d_ploop = nullptr;  // one loop state per instance
 };

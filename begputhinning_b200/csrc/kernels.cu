@@ -816,7 +816,51 @@ __device__ __forceinline__ uint32_t *align128(uint32_t *p)
     return reinterpret_cast<uint32_t *>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
 }
 
+__device__ __forceinline__ void plain_pass_body(Inst *pin, int q, int *flag, int *err);
+
 __global__ void __launch_bounds__(kThreads) plain_pass_kernel(Inst *pin, int q, int *flag, int *err)
+{
+    plain_pass_body(pin, q, flag, err);
+}
+
+// The plain path's pass loop kept on the device: pass q and the change flag
+// live in device memory, and plain_loop_step_kernel decides whether another
+// pass follows (the conditional node of a CUDA graph repeats the pass while
+// it says so), with the same rule as the host loop of run_plain.
+__global__ void __launch_bounds__(kThreads) plain_pass_dev_kernel(Inst *pin, PlainLoop *L, int *err)
+{
+    plain_pass_body(pin, L->q, &L->flag, err);
+}
+
+__global__ void plain_loop_init_kernel(PlainLoop *L)
+{
+    L->q = 0;
+    L->last_change = -1;
+    L->flag = 0;
+    L->converged = 0;
+}
+
+__global__ void plain_loop_step_kernel(PlainLoop *L, Inst *pin, int *err, cudaGraphConditionalHandle h)
+{
+    Inst &in = *pin;
+    const int q = L->q;
+    if (L->flag) L->last_change = q;
+    L->flag = 0;
+    bool done;
+    if (in.dims == 2) done = q - L->last_change >= in.window;
+    else done = q % 6 == 5 && L->last_change < q - 5;
+    L->q = q + 1;
+    if (done) L->converged = 1;
+    else if (q + 1 >= in.pass_cap) {
+        L->converged = -1;
+        atomicOr(err, kErrPassLimit);
+    }
+    in.passes_run = q + 1;
+    in.converged = L->converged;
+    cudaGraphSetConditional(h, L->converged == 0 ? 1u : 0u);
+}
+
+__device__ __forceinline__ void plain_pass_body(Inst *pin, int q, int *flag, int *err)
 {
     extern __shared__ __align__(128) uint32_t smem_raw[];
     uint32_t *smem = align128(smem_raw);
@@ -855,6 +899,27 @@ __global__ void __launch_bounds__(kThreads) plain_pass_kernel(Inst *pin, int q, 
             atomicExch(flag, 1);
         }
     }
+}
+
+cudaError_t launch_plain_dev_pass(int cfg, Inst *d_inst, int ntiles, PlainLoop *d_loop, int *d_err, cudaStream_t st)
+{
+    const CfgInfo *c = cfg_info(cfg);
+    if (!c) return cudaErrorInvalidValue;
+    plain_pass_dev_kernel<<<ntiles, kThreads, c->smem + 128, st>>>(d_inst, d_loop, d_err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plain_loop_init(PlainLoop *d_loop, cudaStream_t st)
+{
+    plain_loop_init_kernel<<<1, 1, 0, st>>>(d_loop);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plain_loop_step(PlainLoop *d_loop, Inst *d_inst, int *d_err, cudaGraphConditionalHandle h,
+                                   cudaStream_t st)
+{
+    plain_loop_step_kernel<<<1, 1, 0, st>>>(d_loop, d_inst, d_err, h);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_plain_pass(int cfg, Inst *d_inst, int ntiles, int q, int *d_flag, int *d_err,
@@ -1303,6 +1368,8 @@ cudaError_t engine_set_smem(int smem)
 {
     cudaError_t e = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          engine_smem_bytes(smem));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(plain_pass_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem + 128);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(plain_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem + 128);
 }

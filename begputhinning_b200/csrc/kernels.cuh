@@ -139,6 +139,20 @@ cudaError_t launch_unpack(int dtype, const uint32_t *buf, int W, int H, int D, i
 cudaError_t launch_tile_init(const Inst *d_inst, const Inst &h_inst, int *d_count, cudaStream_t st);
 cudaError_t launch_plain_pass(int cfg, Inst *d_inst, int ntiles, int q, int *d_flag, int *d_err,
                               cudaStream_t st);
+// Device-side pass loop of the plain path (one per instance).
+struct PlainLoop {
+    int q;            // pass to run next
+    int last_change;  // last pass with a change
+    int flag;         // set by the pass when a tile changed
+    int converged;    // 1 converged, -1 pass cap, 0 running
+};
+cudaError_t launch_plain_dev_pass(int cfg, Inst *d_inst, int ntiles, PlainLoop *d_loop, int *d_err, cudaStream_t st);
+cudaError_t launch_plain_loop_init(PlainLoop *d_loop, cudaStream_t st);
+// Records the pass in the loop state and in the instance (passes_run,
+// converged; kErrPassLimit in *d_err at the cap) and sets the graph's
+// conditional to 1 while another pass is needed.
+cudaError_t launch_plain_loop_step(PlainLoop *d_loop, Inst *d_inst, int *d_err, cudaGraphConditionalHandle h,
+                                   cudaStream_t st);
 cudaError_t launch_engine(int grid, int smem, Inst *d_insts, int ninst, Sched *d_sched, cudaStream_t st);
 cudaError_t launch_rule_table(int dims, int dir, uint32_t *d_out, cudaStream_t st);
 int engine_max_blocks_per_sm(int smem);

@@ -361,6 +361,22 @@ def run_bgt(args, rank, world, local):
         plain = {"value": units / plain_s / 1e6, "unit": UNIT, "ms_per_step": plain_s * 1e3,
                  "what": "one launch per pass per instance, host readback of the change flag after each pass; "
                          "fastest of 3 runs after one untimed run"}
+        # the same passes with the loop on the device: a graph with one
+        # conditional WHILE node per instance (the first run builds it)
+        dl_runs = []
+        for k in range(4):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.run(plain=True, device_loop=True, sync=True)
+            if k > 0:
+                dl_runs.append(time.perf_counter() - t0)
+        dl_s = min(dl_runs)
+        if not torch.equal(dev_out.cpu(), host_out):
+            raise SystemExit("plain path (device loop) output differs from the engine")
+        plain["device_loop"] = {"value": units / dl_s / 1e6, "unit": UNIT, "ms_per_step": dl_s * 1e3,
+                                "what": "the same passes, one CUDA graph with a conditional WHILE node per "
+                                        "instance (no host readback); fastest of 3 replays after the run "
+                                        "that builds the graph"}
 
     # cross-rank aggregation: max time, summed units
     t = torch.tensor([ms, e2e_ms, statistics.median(eng_ms)], device=dev, dtype=torch.float64)

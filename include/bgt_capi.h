@@ -154,7 +154,10 @@ int bgt_batch_set_grid(bgt_batch *b, int ctas);
 int bgt_batch_set_io(bgt_batch *b, int id, int dtype, const void *d_in, void *d_out);
 /* mode 0: persistent engine (optionally replayed as a CUDA graph when
  * use_graph != 0); mode 1: plain path, one launch per pass per instance with
- * a host readback of the change flag after every pass. */
+ * a host readback of the change flag after every pass; mode 2: the same
+ * passes with the loop on the device (a CUDA graph with one conditional
+ * WHILE node per instance, built on the first run and replayed; use_graph is
+ * ignored), so no pass waits for the host. */
 int bgt_batch_run(bgt_batch *b, int mode, int use_graph);
 /* per-instance passes run and whether it converged (1) / hit the cap (-1) */
 int bgt_batch_instance_stats(bgt_batch *b, int id, int *passes, int *converged, int *cfg);

@@ -45,7 +45,7 @@ def _run_batch(ctx, imgs, cfg, plain):
     outs = [torch.empty_like(t) for t in ins]
     for i, t, o in zip(ids, ins, outs):
         b.set_io(i, t, o)
-    b.run(plain=plain)
+    b.run(plain=bool(plain), device_loop=plain == "device")
     torch.cuda.synchronize()
     res = [o.cpu().numpy() for o in outs]
     stats = [b.stats(i) for i in ids]
@@ -53,7 +53,7 @@ def _run_batch(ctx, imgs, cfg, plain):
     return res, stats
 
 
-@pytest.mark.parametrize("plain", [False, True])
+@pytest.mark.parametrize("plain", [False, True, "device"])
 def test_thin2d_all_cfgs(ctx, plain):
     from begputhinning_b200 import cfg_list
     imgs = _cases2d()
@@ -65,7 +65,7 @@ def test_thin2d_all_cfgs(ctx, plain):
         assert all(s["converged"] == 1 for s in stats), (cfg, stats)
 
 
-@pytest.mark.parametrize("plain", [False, True])
+@pytest.mark.parametrize("plain", [False, True, "device"])
 def test_thin3d_all_cfgs(ctx, plain):
     from begputhinning_b200 import cfg_list
     vols = _cases3d()
@@ -75,6 +75,37 @@ def test_thin3d_all_cfgs(ctx, plain):
         for k, (g, w) in enumerate(zip(got, want)):
             assert np.array_equal(g, w), f"cfg {cfg} case {k} shape {vols[k].shape}: {(g != w).sum()} vx differ"
         assert all(s["converged"] == 1 for s in stats), (cfg, stats)
+
+
+def test_plain_device_loop_matches_host_loop(ctx):
+    """The plain path with its pass loop on the device runs the same passes
+    as the host-driven loop (same pass counts), and its graph replays: the
+    second and third runs start from fresh inputs again."""
+    import torch
+    from begputhinning_b200 import Batch
+    rng = np.random.default_rng(12)
+    items = [blobs2d(rng, 300, 420, 40), random2d(rng, 97, 131, 0.5), blobs3d(rng, 30, 40, 50, 5),
+             random3d(rng, 20, 33, 35, 0.5), np.zeros((9, 9), np.uint8), blobs2d(rng, 1100, 900, 300)]
+    want = [po.thin2d(it)[0] if it.ndim == 2 else po.thin3d(it)[0] for it in items]
+    b = Batch(ctx)
+    ids = [b.add(it.shape) for it in items]
+    b.finalize()
+    ins = [torch.from_numpy(it).cuda() for it in items]
+    outs = [torch.empty_like(t) for t in ins]
+    for i, t, o in zip(ids, ins, outs):
+        b.set_io(i, t, o)
+    b.run(plain=True)
+    host = [b.stats(i) for i in ids]
+    for r in range(3):
+        for o in outs:
+            o.fill_(7)
+        b.run(plain=True, device_loop=True)
+        for k, (o, w) in enumerate(zip(outs, want)):
+            assert np.array_equal(o.cpu().numpy(), w), f"run {r} instance {k}"
+        dev = [b.stats(i) for i in ids]
+        assert [s["passes"] for s in dev] == [s["passes"] for s in host]
+        assert all(s["converged"] == 1 for s in dev)
+    b.close()
 
 
 def test_mixed_batch_engine(ctx):
