@@ -79,8 +79,7 @@ def build_lib(verbose: bool = False, ptxas_info: bool = False, force: bool = Fal
         log.append(_run(cmd, verbose))
         objs.append(o)
     tmp = LIB + ".tmp"
-    _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda"] if False else
-         [NVCC, *ARCH, "-shared", "-o", tmp, *objs], verbose)
+    _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs], verbose)
     os.replace(tmp, LIB)
     with open(stamp, "w") as f:
         f.write(dig)

@@ -63,7 +63,11 @@ __host__ __device__ inline size_t up16(size_t v) { return (v + 15) & ~size_t(15)
 }  // namespace
 
 // ------------------------------------------------------------ geometry ----
-constexpr int kUnitRowsH = 24, kUnitWordsH = 8;  // 2D unit (see the 2D section)
+#ifndef BGT_RES_LANE_ROWS
+#define BGT_RES_LANE_ROWS 1
+#endif
+constexpr int kLaneRows = BGT_RES_LANE_ROWS;  // rows of a 2D unit per lane (1 or 2)
+constexpr int kUnitRowsH = 32 * kLaneRows - 8, kUnitWordsH = 8;  // 2D unit (see the 2D section)
 
 // words of shared memory a 2D band of nrows rows needs: zero row, two row
 // copies and the activity record of its units
@@ -159,12 +163,75 @@ __device__ int res_block_exscan(int v, int *total)
 // A pass is one iteration (N, S, E, W) run on register tiles: a warp loads a
 // unit -- 24 core rows plus 4 halo rows above and below (lane = row) by 8
 // core words plus one halo word on either side -- from the pass-start copy,
-// runs the four subiterations in registers (run_subits2d: rows above and
-// below by shuffles, x-neighbours by funnel shifts) and writes its core to
-// the other copy.  Wrong values entering at a unit's edge move one row (or
-// bit) per subiteration, so after four they reach only its halo.
-constexpr int kUnitRows = 32 - 2 * 4;  // core rows of a unit (K = 4)
-constexpr int kUnitWords = 8;          // core words of a unit
+// runs the four subiterations in registers (rows above and below by
+// shuffles, x-neighbours by funnel shifts) and writes its core to the other
+// copy.  Wrong values entering at a unit's edge move one row (or bit) per
+// subiteration, so after four they reach only its halo.
+// BGT_RES_LANE_ROWS=2 builds units of 56 core rows, two adjacent rows per
+// lane (each other's vertical neighbours, half the shuffles per row, less
+// halo): measured slower on stroke images (1.13 against 1.06 ms for 512
+// images), as the larger units stay active for longer.
+constexpr int kUnitRows = 32 * kLaneRows - 2 * 4;  // core rows of a unit (K = 4)
+constexpr int kUnitWords = 8;                      // core words of a unit
+constexpr int kHaloLanes = 4 / kLaneRows;          // lanes holding the top (or bottom) halo rows
+
+// The rule on word j of a lane's two rows a (upper) and b (lower): o the
+// words, n/p the words after/before them (pass-start values).
+template <int DIR>
+__device__ __forceinline__ void word2d_pair(uint32_t oa, uint32_t na, uint32_t pa, uint32_t ob, uint32_t nb,
+                                            uint32_t pb, uint32_t &ra, uint32_t &rb)
+{
+    const uint32_t xpa = at_xp1(oa, na), xma = at_xm1(oa, pa);
+    const uint32_t xpb = at_xp1(ob, nb), xmb = at_xm1(ob, pb);
+    uint32_t A[8], B[8];
+    A[0] = __shfl_up_sync(kFull, ob, 1);   // row above a: the lower row of the lane above
+    A[1] = __shfl_up_sync(kFull, xpb, 1);
+    A[7] = __shfl_up_sync(kFull, xmb, 1);
+    A[2] = xpa;
+    A[6] = xma;
+    A[4] = ob;
+    A[3] = xpb;
+    A[5] = xmb;
+    B[4] = __shfl_down_sync(kFull, oa, 1);  // row below b: the upper row of the lane below
+    B[3] = __shfl_down_sync(kFull, xpa, 1);
+    B[5] = __shfl_down_sync(kFull, xma, 1);
+    B[2] = xpb;
+    B[6] = xmb;
+    B[0] = oa;
+    B[1] = xpa;
+    B[7] = xma;
+    ra = keep2d<DIR>(oa, A);
+    rb = keep2d<DIR>(ob, B);
+}
+
+// One subiteration on the lane's two rows of S+2 words (words j0..j1-1 are
+// processed; the rest keep their values).  Words that are empty in both
+// rows of every lane are skipped.
+template <int S, int DIR, int J0, int J1>
+__device__ __forceinline__ void subit2d_pair(uint32_t (&a)[S + 2], uint32_t (&b)[S + 2])
+{
+    uint32_t pa = J0 > 0 ? a[J0 - 1] : 0u, pb = J0 > 0 ? b[J0 - 1] : 0u;
+#pragma unroll
+    for (int j = J0; j < J1; j++) {
+        const uint32_t oa = a[j], ob = b[j];
+        const uint32_t na = j + 1 < S + 2 ? a[j + 1] : 0u, nb = j + 1 < S + 2 ? b[j + 1] : 0u;
+        if (__any_sync(kFull, (oa | ob) != 0u)) word2d_pair<DIR>(oa, na, pa, ob, nb, pb, a[j], b[j]);
+        pa = oa;
+        pb = ob;
+    }
+}
+
+// K subiterations from phase PH; the last one only on the core words.
+template <int K, int S, int PH, int I = 0>
+__device__ __forceinline__ void run_subits2d_pair(uint32_t (&a)[S + 2], uint32_t (&b)[S + 2])
+{
+    if constexpr (I + 1 < K) {
+        subit2d_pair<S, (PH + I) & 3, 0, S + 2>(a, b);
+        run_subits2d_pair<K, S, PH, I + 1>(a, b);
+    } else if constexpr (I + 1 == K) {
+        subit2d_pair<S, (PH + I) & 3, 1, S + 1>(a, b);
+    }
+}
 
 __host__ __device__ inline int res_pitch2d_tiles(int W)
 {
@@ -204,26 +271,39 @@ __device__ uint32_t res_pass2d(const Band2D &b, int q, int *take, unsigned long 
         if (u >= nunits) break;
         if (b.until[u] < q) continue;
         const int s = u / b.nchunks, c = u - s * b.nchunks;
-        const int r = kUnitRows * s - 4 + lane;
-        const bool valid = r >= 0 && r < b.nrows;
-        const uint32_t *in = valid ? IN + (size_t)r * b.pp : b.zero;
         const int x0 = 1 + kUnitWords * c;
-        uint32_t v[kUnitWords + 2];
+        const int rbase = kUnitRows * s - 4 + kLaneRows * lane;  // band row of the lane's first row
+        uint32_t v[kLaneRows][kUnitWords + 2];
+        const uint32_t *in[kLaneRows];
+        bool valid[kLaneRows];
 #pragma unroll
-        for (int k = 0; k < kUnitWords + 2; k++) v[k] = in[x0 - 1 + k];
-        run_subits2d<4, kUnitWords, 0>(v);
-        const bool mine = valid && lane >= 4 && lane < 4 + kUnitRows;
+        for (int i = 0; i < kLaneRows; i++) {
+            const int r = rbase + i;
+            valid[i] = r >= 0 && r < b.nrows;
+            in[i] = valid[i] ? IN + (size_t)r * b.pp : b.zero;
+#pragma unroll
+            for (int k = 0; k < kUnitWords + 2; k++) v[i][k] = in[i][x0 - 1 + k];
+        }
+        if constexpr (kLaneRows == 2) run_subits2d_pair<4, kUnitWords, 0>(v[0], v[1]);
+        else run_subits2d<4, kUnitWords, 0>(v[0]);
+        const bool core_lane = lane >= kHaloLanes && lane < 32 - kHaloLanes;
         uint32_t chg = 0, lft = 0, rgt = 0;
-        if (mine) {
-            uint32_t *out = OUT + (size_t)r * b.pp;
+#pragma unroll
+        for (int i = 0; i < kLaneRows; i++) {
+            if (!(valid[i] && core_lane)) continue;
+            uint32_t *out = OUT + (size_t)(rbase + i) * b.pp;
+            uint32_t ci = 0;
 #pragma unroll
             for (int k = 0; k < kUnitWords; k++) {
-                const uint32_t d = v[1 + k] ^ in[x0 + k];
-                chg |= d;
-                if (k == 0) lft = d & 0xFu;                     // within 4 pixels of the left edge
-                if (k == kUnitWords - 1) rgt = d & 0xF0000000u;  // ... of the right edge
-                out[x0 + k] = v[1 + k];
+                const uint32_t d = v[i][1 + k] ^ in[i][x0 + k];
+                ci |= d;
+                if (k == 0) lft |= d & 0xFu;                     // within 4 pixels of the left edge
+                if (k == kUnitWords - 1) rgt |= d & 0xF0000000u;  // ... of the right edge
+                out[x0 + k] = v[i][1 + k];
             }
+            chg |= ci;
+            const int gy = b.a + rbase + i;
+            if (gy >= b.r0 && gy < b.r1) core |= ci;
         }
         // The next pass of a neighbour depends on this unit only through the
         // 4 pixels next to their common border (four subiterations reach 4
@@ -232,7 +312,9 @@ __device__ uint32_t res_pass2d(const Band2D &b, int q, int *take, unsigned long 
         const unsigned m_any = __ballot_sync(kFull, chg != 0u);
         if (m_any) {
             const unsigned m_l = __ballot_sync(kFull, lft != 0u), m_r = __ballot_sync(kFull, rgt != 0u);
-            const unsigned band_top = 0x000000F0u, band_bot = 0x0F000000u;  // lanes 4..7, 24..27
+            // lanes holding the first and last 4 core rows
+            constexpr unsigned band_top = ((1u << kHaloLanes) - 1u) << kHaloLanes;
+            constexpr unsigned band_bot = ((1u << kHaloLanes) - 1u) << (32 - 2 * kHaloLanes);
             if (lane < 9) {
                 const int dy = lane / 3 - 1, dx = lane % 3 - 1;
                 const unsigned rows = dy < 0 ? band_top : dy > 0 ? band_bot : ~0u;
@@ -242,9 +324,6 @@ __device__ uint32_t res_pass2d(const Band2D &b, int q, int *take, unsigned long 
                     b.until[ns * b.nchunks + nc] = q + 1;
             }
         }
-
-        const int gy = b.a + r;
-        if (mine && gy >= b.r0 && gy < b.r1) core |= chg;
         if (lane == 0)
             *words += (unsigned long long)min(kUnitRows, b.nrows - kUnitRows * s) *
                       min(kUnitWords, b.wl - kUnitWords * c);

@@ -52,6 +52,46 @@ __device__ __forceinline__ uint32_t rule2d(const uint32_t (&X)[8])
                           X[(5 + r) & 7], X[(6 + r) & 7], X[(7 + r) & 7]);
 }
 
+// d = f(a, b, c) for the three-input function with truth table IMM
+// (bit 4a + 2b + c of IMM), one LOP3 instruction.
+template <unsigned IMM>
+__device__ __forceinline__ uint32_t lop3(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("lop3.b32 %0, %1, %2, %3, %4;" : "=r"(d) : "r"(a), "r"(b), "r"(c), "n"(IMM));
+    return d;
+}
+
+// The centre word o after one subiteration of direction S: o & ~rule2d<S>.
+// Written as eleven three-input operations (the factored template above,
+// with the select on x2 for G0 and the final keep folded in); the two forms
+// agree on all 512 (centre, ring) combinations.
+#ifndef BGT_RULE2D_LOP3
+#define BGT_RULE2D_LOP3 1
+#endif
+template <int S>
+__device__ __forceinline__ uint32_t keep2d(uint32_t o, const uint32_t (&X)[8])
+{
+#if BGT_RULE2D_LOP3
+    constexpr int r = rot2d(S);
+    const uint32_t x0 = X[(0 + r) & 7], x1 = X[(1 + r) & 7], x2 = X[(2 + r) & 7], x3 = X[(3 + r) & 7];
+    const uint32_t x4 = X[(4 + r) & 7], x5 = X[(5 + r) & 7], x6 = X[(6 + r) & 7], x7 = X[(7 + r) & 7];
+    const uint32_t h = lop3<0xD0>(x4, x2, x1);   // x4 & (x2 | ~x1)
+    const uint32_t t = lop3<0xFE>(x1, x3, x4);   // x1 | x3 | x4
+    const uint32_t q = lop3<0x08>(x1, x3, x4);   // ~x1 & x3 & x4
+    const uint32_t a = lop3<0xF4>(x6, x5, x7);   // x6 | (x5 & ~x7)
+    const uint32_t b = lop3<0xE0>(x6, x5, x7);   // x6 & (x5 | x7)
+    const uint32_t c = lop3<0x01>(x5, x6, x7);   // ~(x5 | x6 | x7)
+    const uint32_t bz = lop3<0x10>(b, t, x2);    // b & ~t & ~x2        (b & Z)
+    const uint32_t g0 = lop3<0xCA>(x2, t, q);    // x2 ? t : q          (G0)
+    const uint32_t ah = lop3<0xEA>(a, h, bz);    // (a & h) | bz
+    const uint32_t tt = lop3<0xF8>(ah, c, g0);   // ah | (c & g0)
+    return lop3<0xD0>(o, x0, tt);                // o & (x0 | ~tt)
+#else
+    return o & ~rule2d<S>(X);
+#endif
+}
+
 // ---------------------------------------------------------------- 3D ------
 // Neighbourhood words g[9*(dz+1) + 3*(dy+1) + (dx+1)] (g[13] = centre).
 // Direction d in application order 0..5 = U, N, E, D, S, W.  In the

@@ -55,7 +55,7 @@ __device__ __forceinline__ uint32_t word2d(uint32_t o, uint32_t n, uint32_t p)
     X[5] = __shfl_down_sync(kFull, xm, 1);
     X[2] = xp;
     X[6] = xm;
-    return o & ~rule2d<DIR>(X);
+    return keep2d<DIR>(o, X);
 }
 
 // One subiteration on the lane's S+2 words, two words per step so that the

@@ -2,7 +2,8 @@
 (begputhinning_b200/csrc/resident.cu: res_run2d, res_pass2d): an image cut
 into bands of rows that each keep `halo` extra rows on both sides; a pass is
 one iteration (N, S, E, W) computed per unit of 24 rows x 8 words on a
-register tile with 4 halo rows and one halo word on either side; a unit is
+register tile with 4 halo rows and one halo word on either side (56 rows in
+the two-rows-per-lane build); a unit is
 processed in the next pass when it changed or a neighbour changed within 4
 pixels of their common border (border bands); the bands run passes in lockstep with a halo exchange after each, and
 stop after a pass without a core deletion in any band.
@@ -135,10 +136,11 @@ def _images():
             random2d(rng, 64, 40, 0.9), blobs2d(rng, 70, 900, 60, rmax=12)]
 
 
+@pytest.mark.parametrize("unit_rows", [24, 56])
 @pytest.mark.parametrize("bands", [1, 2, 3, 5])
-def test_band_model_matches_oracle(bands):
+def test_band_model_matches_oracle(bands, unit_rows):
     for img in _images():
-        got, _ = run_band_model(img, bands)
+        got, _ = run_band_model(img, bands, unit_rows=unit_rows)
         assert np.array_equal(got, po.thin2d(img)[0]), (img.shape, bands)
 
 
