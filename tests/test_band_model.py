@@ -5,8 +5,10 @@ one iteration (N, S, E, W) computed per unit of 24 rows x 8 words on a
 register tile with 4 halo rows and one halo word on either side (56 rows in
 the two-rows-per-lane build); a unit is
 processed in the next pass when it changed or a neighbour changed within 4
-pixels of their common border (border bands); the bands run passes in lockstep with a halo exchange after each, and
-stop after a pass without a core deletion in any band.
+pixels of their common border (border bands); the bands run passes in
+lockstep with a halo exchange after every second pass (8 halo rows: two
+passes move wrong values in from a band's edge by at most 8 rows), and stop
+after an exchange pass without a core deletion in any band.
 Deletions use the oracle's rule table, so the model checks the protocol and
 its exactness argument, not the device's arithmetic: it must reproduce the
 oracle's thinning on every image, and it must fail when the halo is too
@@ -59,7 +61,7 @@ def run_tile(rows, r0, r1, c0, c1):
     return t[4:4 + (r1 - r0), 32:32 + (c1 - c0)]
 
 
-def run_band_model(img, bands, halo=4, unit_rows=24, unit_px=8 * 32):
+def run_band_model(img, bands, halo=8, unit_rows=24, unit_px=8 * 32, every=2):
     H, W = img.shape
     state = img.copy()  # global buffer (the bands' boundary rows are traded through it)
     cuts = [k * H // bands for k in range(bands + 1)]
@@ -114,6 +116,8 @@ def run_band_model(img, bands, halo=4, unit_rows=24, unit_px=8 * 32):
             if not any_core:
                 return B[0]["rows"], q + 1
             continue
+        if q % every != every - 1:
+            continue  # the bands meet after every `every` passes
         for bd in B:  # core rows -> global
             state[bd["r0"]:bd["r1"]] = bd["rows"][bd["r0"] - bd["a"]:bd["r1"] - bd["a"]]
         if not any_core:
@@ -144,11 +148,22 @@ def test_band_model_matches_oracle(bands, unit_rows):
         assert np.array_equal(got, po.thin2d(img)[0]), (img.shape, bands)
 
 
-def test_band_model_needs_its_halo():
-    """With halo rows thinner than one iteration's reach (4 subiterations)
-    some image comes out wrong: the model can tell a broken protocol."""
-    wrong = 0
+def test_band_model_exchange_every_pass():
+    """The earlier protocol: 4 halo rows, an exchange after every pass."""
     for img in _images():
-        got, _ = run_band_model(img, 3, halo=1)
-        wrong += not np.array_equal(got, po.thin2d(img)[0])
+        got, _ = run_band_model(img, 3, halo=4, every=1)
+        assert np.array_equal(got, po.thin2d(img)[0]), img.shape
+
+
+@pytest.mark.parametrize("halo,every", [(1, 1), (3, 2)])
+def test_band_model_needs_its_halo(halo, every):
+    """With halo rows thinner than the reach of the passes between two
+    exchanges (4 rows per pass) some image comes out wrong: the model can
+    tell a broken protocol."""
+    wrong = 0
+    rng = np.random.default_rng(11)
+    for img in _images() + [random2d(rng, 160, 90, 0.8), blobs2d(rng, 240, 100, 30, rmax=20)]:
+        for bands in (2, 3):
+            got, _ = run_band_model(img, bands, halo=halo, every=every)
+            wrong += not np.array_equal(got, po.thin2d(img)[0])
     assert wrong > 0
