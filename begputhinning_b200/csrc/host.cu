@@ -253,7 +253,7 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // of one image consecutive.
 static void plan_resident(bgt_batch *b)
 {
-    constexpr int kHalo = 8, kMinCore = 32;  // 2D band halo: two passes between exchanges
+    constexpr int kHalo = kResHalo2D, kMinCore = 32;  // 2D band halo
     b->res_items.clear();
     b->any_ring = false;
     b->any_res3d = false;

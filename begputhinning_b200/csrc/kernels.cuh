@@ -68,6 +68,14 @@ struct ResTrace {
     long long t0, t1;
     int sm, pad;
 };
+// 2D bands of one image meet every kResPassesPerExchange passes; wrong
+// values entering at a band's edge move at most 4 rows per pass, so the
+// bands keep 4 halo rows per pass of the period
+#ifndef BGT_RES_PASSES_PER_EXCHANGE
+#define BGT_RES_PASSES_PER_EXCHANGE 4  // measured: 1, 2, 3, 4 -> mixed batch 1.20, 1.11, 1.10, 1.09 ms
+#endif
+constexpr int kResPassesPerExchange = BGT_RES_PASSES_PER_EXCHANGE;
+constexpr int kResHalo2D = 4 * kResPassesPerExchange;
 constexpr int kResThreads = 768;
 constexpr int kResCtasPerSm = 1;
 constexpr int kResSmemBytes = 230400;  // dynamic shared memory of one CTA (one per SM)

@@ -22,13 +22,14 @@
 // single band stops after four consecutive subiterations without a deletion
 // (a fixed point of N, S, E and W: the reference's result, whatever the
 // alignment).  Bands of one image run their iterations (N, S, E, W) in
-// lockstep, meeting after every second one: then a band writes its first and
-// last `halo` core rows to global memory, meets the other bands at a
-// per-image counter, stops if no band's core changed in that iteration, and
-// otherwise reads its halo rows from its neighbours.  With halo = 8 rows,
-// wrong values entering at a band's outer edge during two iterations (4 rows
-// each at most) reach at most its halo rows; if the iteration before the
-// meeting was already a fixed point, the one at the meeting is too.
+// lockstep, meeting after every kResPassesPerExchange-th one: then a band
+// writes its first and last `halo` core rows to global memory, meets the
+// other bands at a per-image counter, stops if no band's core changed in
+// that iteration, and otherwise reads its halo rows from its neighbours.
+// With halo = 4 rows per iteration of the period, wrong values entering at a
+// band's outer edge between two meetings (4 rows per iteration at most)
+// reach at most its halo rows; if an iteration before the meeting was
+// already a fixed point, the one at the meeting is too.
 //
 // 3D volume (sparse bricks, one CTA).  Deletion never adds foreground, so
 // bricks of 32 voxels (one word) x 32 rows x 4 planes that are empty at the
@@ -173,7 +174,6 @@ __device__ int res_block_exscan(int v, int *total)
 // lane (each other's vertical neighbours, half the shuffles per row, less
 // halo): measured slower on stroke images (1.13 against 1.06 ms for 512
 // images), as the larger units stay active for longer.
-constexpr int kPassesPerExchange = 2;              // passes between the halo exchanges of a band
 constexpr int kUnitRows = 32 * kLaneRows - 2 * 4;  // core rows of a unit (K = 4)
 constexpr int kUnitWords = 8;                      // core words of a unit
 constexpr int kHaloLanes = 4 / kLaneRows;          // lanes holding the top (or bottom) halo rows
@@ -387,11 +387,11 @@ __device__ void res_run2d(Inst &in, const ResItem &it, uint32_t *sm, ResSched *S
                 result = 1;
                 break;
             }
-        } else if (q % kPassesPerExchange == kPassesPerExchange - 1) {
+        } else if (q % kResPassesPerExchange == kResPassesPerExchange - 1) {
             // end of pass q (state in buf[(q+1)&1]), the last of an exchange
             // period: trade boundary rows with the neighbouring bands
             const int h = it.halo;
-            const int e = q / kPassesPerExchange;  // exchange index
+            const int e = q / kResPassesPerExchange;  // exchange index
             uint32_t *cur = (q & 1) ? b.buf0 : b.buf1;
             uint32_t *gx = in.buf[(e + 1) & 1];  // buf[0] holds the start state other bands may still load
             for (int k = warp; k < 2 * h; k += kWarps) {

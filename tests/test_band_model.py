@@ -6,8 +6,8 @@ register tile with 4 halo rows and one halo word on either side (56 rows in
 the two-rows-per-lane build); a unit is
 processed in the next pass when it changed or a neighbour changed within 4
 pixels of their common border (border bands); the bands run passes in
-lockstep with a halo exchange after every second pass (8 halo rows: two
-passes move wrong values in from a band's edge by at most 8 rows), and stop
+lockstep with a halo exchange after every fourth pass (16 halo rows: four
+passes move wrong values in from a band's edge by at most 16 rows), and stop
 after an exchange pass without a core deletion in any band.
 Deletions use the oracle's rule table, so the model checks the protocol and
 its exactness argument, not the device's arithmetic: it must reproduce the
@@ -61,7 +61,7 @@ def run_tile(rows, r0, r1, c0, c1):
     return t[4:4 + (r1 - r0), 32:32 + (c1 - c0)]
 
 
-def run_band_model(img, bands, halo=8, unit_rows=24, unit_px=8 * 32, every=2):
+def run_band_model(img, bands, halo=16, unit_rows=24, unit_px=8 * 32, every=4):
     H, W = img.shape
     state = img.copy()  # global buffer (the bands' boundary rows are traded through it)
     cuts = [k * H // bands for k in range(bands + 1)]
@@ -141,10 +141,11 @@ def _images():
 
 
 @pytest.mark.parametrize("unit_rows", [24, 56])
+@pytest.mark.parametrize("halo,every", [(16, 4), (8, 2)])
 @pytest.mark.parametrize("bands", [1, 2, 3, 5])
-def test_band_model_matches_oracle(bands, unit_rows):
+def test_band_model_matches_oracle(bands, halo, every, unit_rows):
     for img in _images():
-        got, _ = run_band_model(img, bands, unit_rows=unit_rows)
+        got, _ = run_band_model(img, bands, halo=halo, every=every, unit_rows=unit_rows)
         assert np.array_equal(got, po.thin2d(img)[0]), (img.shape, bands)
 
 
