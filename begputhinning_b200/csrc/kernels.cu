@@ -521,8 +521,12 @@ __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__
             ke = k + 1 < n ? io[k + 1].wbegin : total;
             const Inst &in = insts[d.inst];
             buf0 = in.buf[0];
-            buf1 = in.buf[1];
-            lc = in.lc;
+            // an image thinned by the resident kernel reads only buf[0] and
+            // no tile marks (its bands write buf[1] before reading it); the
+            // tile engine and volumes, which may spill to it, need both
+            const bool res2d = in.res && in.dims == 2;
+            buf1 = res2d ? nullptr : in.buf[1];
+            lc = res2d ? nullptr : in.lc;
             P = in.P;
             H = in.H;
             tiles_x = in.tiles_x;
@@ -560,6 +564,7 @@ __global__ void pack_all_kernel(const Inst *__restrict__ insts, const IODesc *__
             }
         }
         buf0[i] = w;
+        if (!buf1) continue;
         buf1[i] = w;
         if (w) {  // tile holds foreground: lc = -1 (pre-filled with kNever)
             const int t = ((int)fdiv(d.dTZ, z) * tiles_y + (int)fdiv(d.dTH, (uint32_t)y)) * tiles_x +
