@@ -1,8 +1,9 @@
 // resident.cu -- the resident engine: every work item (an instance, or one
 // band of rows of a 2D image too large for one CTA) is loaded once into one
 // CTA's shared memory and thinned there from its first subiteration to its
-// fixed point; only the bands of a large image (or slabs of a large volume)
-// meet, once per iteration, to trade boundary rows through global memory.
+// fixed point; only the bands of a large image (every fourth iteration) and
+// the slabs of a large volume (every iteration) meet to trade boundary rows
+// through global memory.
 // One CTA of 768 threads per SM holds up to 225 KB (measured against two
 // CTAs of 384 threads with 111 KB each: larger bands and slabs won).
 //

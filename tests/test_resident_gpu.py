@@ -61,7 +61,8 @@ def test_resident_images_single_cta(ctx):
                                        ((333, 70), False), ((97, 4000), True)])
 def test_resident_image_bands(ctx, shape, cut):
     """One image per batch: the planner cuts it into bands (at least 32 core
-    rows each) that run on separate CTAs and meet after every iteration."""
+    rows each) that run on separate CTAs and meet after every fourth
+    iteration to trade 16 halo rows."""
     rng = np.random.default_rng(sum(shape))
     h, w = shape
     img = blobs2d(rng, h, w, max(1, h * w // 1500), rmax=14)
